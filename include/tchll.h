@@ -1,0 +1,243 @@
+/*
+ * tchll.h -- C ABI of libtchll, the B200 (sm_100a) implementation of the
+ * hybrid exact / HyperLogLog triangle-counting path of
+ * ChitandaEruQ/triangle_counting_hll.
+ *
+ * Conventions
+ *   - Every pointer argument is DEVICE memory unless its comment says "host".
+ *   - Nothing here allocates device memory.  Scratch comes from a caller
+ *     buffer ("workspace") whose size the matching *_workspace_bytes query
+ *     returns; a NULL workspace is never dereferenced by the query.
+ *   - `stream` is a cudaStream_t (NULL = legacy default stream).  All work is
+ *     stream-ordered; results written to device memory are valid once the
+ *     stream has been synchronised.  No call synchronises except where noted.
+ *   - Every function returns TCHLL_OK (0) or an error code; the message of the
+ *     last error on the calling thread is tchll_last_error().
+ *   - Ids and CSR offsets are int32, as in the reference (src/gpu_graph.py:6-41).
+ *
+ * Each declaration names the reference interface it replaces (file:line in
+ * the reference project).
+ */
+#ifndef TCHLL_H
+#define TCHLL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TCHLL_OK 0
+#define TCHLL_EINVAL 1     /* invalid argument (the reference raises ValueError) */
+#define TCHLL_ECUDA 2      /* CUDA runtime error */
+#define TCHLL_EWORKSPACE 3 /* workspace smaller than the query returned */
+
+/* Malformed-input flags a kernel reports in tchll_count_result.status. */
+#define TCHLL_STATUS_BAD_EDGE 1u /* edge endpoint outside [0, n_nodes) */
+#define TCHLL_STATUS_BAD_ROW 2u  /* row_ptr extent outside [0, nnz] or decreasing */
+#define TCHLL_STATUS_BAD_SLOT 4u /* sketch slot outside [0, n_rows) */
+
+/*
+ * Totals written by the counting entry points (64 bytes, device memory).
+ * exact      sum of exact supports over exact-routed edges (uint64, exact)
+ * hll_fx     sum of clamped HLL supports in fixed point, units of 2^-32,
+ *            as a 128-bit integer (hll_fx_hi:hll_fx_lo); each edge's clamped
+ *            FP64 estimate is rounded to the nearest 2^-32 before summing, so
+ *            the total is independent of summation order
+ * n_*        the reference's stats (src/hybrid.py:152-164,
+ *            src/gpu_hybrid.py:415-430); n_fallback counts edges that wanted
+ *            HLL but lacked a sketch on one side
+ * status     TCHLL_STATUS_* flags; non-zero means the input was malformed and
+ *            the offending edges were skipped
+ */
+typedef struct tchll_count_result {
+    uint64_t exact;
+    uint64_t hll_fx_lo;
+    uint64_t hll_fx_hi;
+    int64_t n_approx;
+    int64_t n_exact;
+    int64_t n_fallback;
+    int64_t n_clamped;
+    uint32_t status;
+    uint32_t reserved;
+} tchll_count_result;
+
+/* ------------------------------------------------------------- library --- */
+const char* tchll_last_error(void);
+int tchll_version(void);
+/* Number of kernels this library has launched in this process (host). */
+uint64_t tchll_launch_count(void);
+
+/* --------------------------------------------- exact / hybrid counting --- */
+/* Workspace for tchll_exact_count / tchll_hybrid_count_*. */
+int tchll_count_workspace_bytes(int64_t n_edges, size_t* bytes);
+
+/*
+ * Exact count: T = sum over the n_edges edges (edge_u[i], edge_v[i]) of
+ * |N+(u) cap N+(v)| with N+(x) = col_idx[row_ptr[x] .. row_ptr[x+1]) (sorted,
+ * duplicate-free).  Replaces gpu_exact_triangle_count
+ * (src/gpu_hybrid.py:332-354) and the loop of exact_triangle_count
+ * (src/exact.py:48-98).  per_edge_support (nullable, n_edges int64) receives
+ * each edge's support.
+ */
+int tchll_exact_count(const int32_t* row_ptr, int64_t n_nodes, const int32_t* col_idx, int64_t nnz,
+                      const int32_t* edge_u, const int32_t* edge_v, int64_t n_edges,
+                      int64_t* per_edge_support, tchll_count_result* result, void* workspace,
+                      size_t workspace_bytes, void* stream);
+
+/*
+ * Hybrid count over DENSE sketches (row v at sketch_regs + v * 2^p, present
+ * iff has_sketch[v] == 1).  An edge goes to HLL iff
+ * min(degrees[u], degrees[v]) >= gamma and both endpoints have a sketch.
+ * split_kernels != 0 runs the exact-routed and HLL-routed edges as two
+ * launches, otherwise one.  Replaces gpu_hybrid_triangle_count
+ * (src/gpu_hybrid.py:357-431).  p outside [4, 16] is TCHLL_EINVAL.
+ */
+int tchll_hybrid_count_dense(const int32_t* row_ptr, int64_t n_nodes, const int32_t* col_idx, int64_t nnz,
+                             const int32_t* edge_u, const int32_t* edge_v, int64_t n_edges,
+                             const int32_t* degrees, const uint8_t* sketch_regs, const uint8_t* has_sketch,
+                             int32_t p, int64_t gamma, int32_t split_kernels, tchll_count_result* result,
+                             void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * Hybrid count over COMPACT sketches: slot[v] >= 0 selects row
+ * rows + slot[v] * 2^p (n_rows rows), -1 means no sketch.  Replaces the loop
+ * of hybrid_triangle_count (src/hybrid.py:48-166).  The four per-edge outputs
+ * (support int64, s_hat f64, s_clamped f64, method u8: 0 exact / 1 HLL) are
+ * all NULL or all set; support is written for exact edges, s_hat/s_clamped
+ * for HLL edges.
+ */
+int tchll_hybrid_count_compact(const int32_t* row_ptr, int64_t n_nodes, const int32_t* col_idx, int64_t nnz,
+                               const int32_t* edge_u, const int32_t* edge_v, int64_t n_edges,
+                               const int32_t* degrees, const uint8_t* rows, int64_t n_rows, const int64_t* slot,
+                               int32_t p, int64_t gamma, int32_t split_kernels, int64_t* per_edge_support,
+                               double* per_edge_s_hat, double* per_edge_s_clamped, uint8_t* per_edge_method,
+                               tchll_count_result* result, void* workspace, size_t workspace_bytes,
+                               void* stream);
+
+/* Launch shape of the counting kernels (host state; no counterpart in the
+ * reference, whose block size is fixed at 256, src/gpu_hybrid.py:13).
+ * chunk: edges claimed per warp (multiple of 32); slots_log2: per-warp hash
+ * table capacity; tiny: lane-local merge threshold on |N+u|+|N+v|;
+ * blocks_per_sm: 0 = occupancy maximum.  out4 receives the same four. */
+int tchll_set_count_tuning(int32_t chunk, int32_t slots_log2, int32_t tiny, int32_t blocks_per_sm);
+int tchll_get_count_tuning(int32_t* out4 /* host */);
+
+/* ------------------------------------------------------------ sketches --- */
+/*
+ * Dense sketch build, launch-compatible with build_sketches_kernel
+ * (src/gpu_hll.py:47-81): for every u, has_sketch[u] = (row length >= theta);
+ * for those u, the registers of N+(u) (hashing the col_idx values) are
+ * max-merged into sketch_regs[u * 2^p ..] (pass zeroed rows for fresh
+ * sketches, as alloc_sketch_arrays does, src/gpu_hll.py:128-133).  Needs no
+ * workspace.
+ */
+int tchll_build_sketches_dense(const int32_t* row_ptr, int64_t n_nodes, const int32_t* col_idx, int64_t nnz,
+                               int64_t theta, int32_t p, uint8_t* sketch_regs, uint8_t* has_sketch, void* stream);
+
+/*
+ * Compact sketches (src/hybrid.py:15-41): tchll_sketch_slots (workspace from
+ * tchll_sketch_workspace_bytes) writes
+ * slot[u] = rank of u among vertices with row length >= theta (ascending u),
+ * or -1, and the number of sketches to *n_sketched (device int64).
+ * tchll_build_sketches_compact then writes rows[slot[u] * 2^p ..] for every
+ * sketched u (rows are overwritten, not merged).  keys (nullable, int64,
+ * n_nodes) maps a column to the value hashed in its place: keys[col_idx[k]]
+ * -- the original vertex ids when the CSR holds compacted ones
+ * (src/hybrid.py:39 hashes forward_adj's ids); NULL hashes col_idx[k].
+ */
+int tchll_sketch_workspace_bytes(int64_t n_nodes, size_t* bytes);
+int tchll_sketch_slots(const int32_t* row_ptr, int64_t n_nodes, int64_t theta, int64_t* slot, int64_t* n_sketched,
+                       void* workspace, size_t workspace_bytes, void* stream);
+int tchll_build_sketches_compact(const int32_t* row_ptr, int64_t n_nodes, const int32_t* col_idx,
+                                 const int64_t* keys, int64_t nnz, const int64_t* slot, int64_t n_rows, int32_t p,
+                                 uint8_t* rows, void* stream);
+
+/* HLL.add_array (src/hll.py:93-96): max-merge the registers of n int64 values
+ * into one row of 2^p registers. */
+int tchll_hll_add(uint8_t* regs, int32_t p, const int64_t* values, int64_t n, void* stream);
+
+/*
+ * Estimates for n_pairs pairs of rows: out[i] = estimate of the register-wise
+ * max of rows[a[i]] and rows[b[i]] (union_estimate, src/hll.py:112-120), or of
+ * rows[a[i]] alone when b is NULL or b[i] < 0 (HLL.estimate, src/hll.py:98-100).
+ */
+int tchll_hll_estimate_pairs(const uint8_t* rows, int64_t n_rows, int32_t p, const int64_t* a, const int64_t* b,
+                             int64_t n_pairs, double* out, void* stream);
+
+/* _hash64 (src/hll.py:13-19) of n int64 values. */
+int tchll_hash64(const int64_t* values, int64_t n, uint64_t* out, void* stream);
+
+/* -------------------------------------------------- CSR construction --- */
+/*
+ * Edge list -> oriented CSR, the array form of orient_graph + to_csr_numpy
+ * (src/graph.py:29-61, src/gpu_graph.py:6-41) as vectorised in
+ * experiment/exp_gpu.py:317-365: canonical (min,max) pairs, self-loops and
+ * duplicates dropped, ids compacted to the rank among all endpoint ids,
+ * undirected degree, orientation u->v iff (deg u, id u) < (deg v, id v),
+ * rows sorted.  Two phases sharing one workspace:
+ *   phase 1 writes sizes[0] = n_nodes, sizes[1] = n_edges (device int64[2]);
+ *   phase 2 (after the caller has read the sizes and allocated the outputs)
+ *   writes row_ptr[n_nodes+1], col_idx/edge_u/edge_v[n_edges],
+ *   degrees (forward)[n_nodes], node_ids (original id)[n_nodes] and, when
+ *   undirected_degrees is not NULL, the undirected degree[n_nodes]
+ *   (orient_graph's degree dict, src/graph.py:41-44).
+ * Negative ids are TCHLL_EINVAL via sizes[0] = -1.
+ */
+int tchll_csr_workspace_bytes(int64_t n_raw, size_t* bytes);
+int tchll_csr_build_phase1(const int32_t* raw_u, const int32_t* raw_v, int64_t n_raw, int64_t* sizes,
+                           void* workspace, size_t workspace_bytes, void* stream);
+int tchll_csr_build_phase2(int64_t n_raw, int64_t n_nodes, int64_t n_edges, int32_t* row_ptr, int32_t* col_idx,
+                           int32_t* degrees, int32_t* node_ids, int32_t* edge_u, int32_t* edge_v,
+                           int32_t* undirected_degrees, void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * forward_adj -> CSR, the device form of to_csr_numpy (src/gpu_graph.py:6-41):
+ * keys[n] (dict order), row lengths lens[n] and the concatenated neighbour
+ * values[nnz] (dict order).  Rows are emitted in ascending key order, each
+ * value replaced by the rank of its key; sizes: node_ids[n], row_ptr[n+1],
+ * degrees[n], col_idx/edge_u/edge_v[nnz], order[n] = dict position of each
+ * emitted row.  *missing (device int64) counts values that are not keys (the
+ * reference raises KeyError).
+ */
+int tchll_adj_workspace_bytes(int64_t n, int64_t nnz, size_t* bytes);
+int tchll_csr_from_adjacency(const int64_t* keys, const int64_t* lens, int64_t n, const int64_t* values,
+                             int64_t nnz, int64_t* node_ids, int32_t* row_ptr, int32_t* degrees, int32_t* col_idx,
+                             int32_t* edge_u, int32_t* edge_v, int64_t* order, int64_t* missing, void* workspace,
+                             size_t workspace_bytes, void* stream);
+
+/* ------------------------------------------------------ text ingest --- */
+/*
+ * Parse whitespace-separated edge-list text (text: device bytes) the way
+ * load_edgelist / the experiment loader read files (src/graph.py:8-26,
+ * experiment/exp_gpu.py:131-144): stripped lines, empty lines and lines whose
+ * first character is in comment_chars (host C string) skipped, lines with
+ * fewer than two tokens skipped, first two tokens parsed as integers.  Pairs
+ * go to out_u/out_v (capacity n_bytes / 4 + 2 suffices: every kept line takes
+ * at least four bytes, the last three); *n_out (device int64) receives their
+ * number and *n_bad the lines whose tokens are not int32 integers (the
+ * reference raises ValueError on those).  Self-loops are kept (the CSR
+ * builder drops them).  Synchronises `stream` once.
+ */
+int tchll_ingest_workspace_bytes(int64_t n_bytes, size_t* bytes);
+int tchll_parse_edges(const uint8_t* text, int64_t n_bytes, const char* comment_chars, int32_t* out_u, int32_t* out_v,
+                      int64_t* n_out, int64_t* n_bad, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ------------------------------------------------ synthetic generators --- */
+/* Seeded generators (no counterpart in the reference, which reads SNAP
+ * files); key(seed,s) = mix((seed+1)*G ^ s*C), draw(key,i) = mix(key+(i+1)*G),
+ * mix = splitmix64 finaliser.  Thresholds are probabilities * 2^32. */
+int tchll_gen_rmat(int32_t scale, int64_t n_raw, uint32_t ta, uint32_t tab, uint32_t tabc, uint64_t seed,
+                   int32_t* u, int32_t* v, void* stream);
+int tchll_gen_er(int64_t n, int64_t n_raw, uint64_t seed, int32_t* u, int32_t* v, void* stream);
+int64_t tchll_gen_lattice_count(int64_t rows, int64_t cols);
+int tchll_gen_lattice(int64_t rows, int64_t cols, uint32_t tdiag, uint32_t tdel, uint64_t seed, int32_t* u,
+                      int32_t* v, void* stream);
+int tchll_gen_chung_lu(const uint64_t* cum, int64_t n, int64_t n_raw, uint64_t seed, int32_t* u, int32_t* v,
+                       void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TCHLL_H */

@@ -1,0 +1,412 @@
+"""GPU parity tests: libtchll (through its C ABI, via the package) against the
+CPU oracle and the golden fixtures recorded from the reference.
+
+Bit-exact: CSR arrays, exact counts, HLL registers, routing stats.
+Tolerance: hybrid totals within 1e-9 relative of the FP64 oracle (the
+north-star bar is 1e-6), single estimates within 1e-12 relative.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+HYB_RTOL = 1e-9
+EST_RTOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def dev(tchll):
+    import torch
+    return torch.device("cuda", 0)
+
+
+def _np(t):
+    return t.cpu().numpy()
+
+
+def _ocsr(O, u, v):
+    return O.csr_build(np.asarray(u), np.asarray(v))
+
+
+def _check_csr(g, og):
+    assert g.n_nodes == og["n_nodes"] and g.n_edges == og["n_edges"]
+    assert np.array_equal(_np(g.row_ptr), og["row_ptr"])
+    assert np.array_equal(_np(g.col_idx), og["col_idx"])
+    assert np.array_equal(_np(g.degrees), og["degrees"])
+    assert np.array_equal(_np(g.node_ids).astype(np.int64), og["node_ids"])
+    assert np.array_equal(_np(g.edge_u), og["edge_u"])
+    assert np.array_equal(_np(g.edge_v), og["edge_v"])
+
+
+def _exact(core, g):
+    res, _ = core.exact_count_tensors(g.row_ptr, g.col_idx, g.edge_u, g.edge_v)
+    return core.exact_from_result(res)
+
+
+# ------------------------------------------------------------ generators
+def test_device_generators_match_oracle(tchll, oracle, dev):
+    from triangle_counting_hll_b200 import core
+    du, dv = core.gen_rmat(14, 16, 0.57, 0.19, 0.19, seed=1, device=dev)
+    ou, ov = oracle.gen_rmat(14, 16, 0.57, 0.19, 0.19, 1)
+    assert np.array_equal(_np(du), ou) and np.array_equal(_np(dv), ov)
+    du, dv = core.gen_er(20000, 100000, seed=0, device=dev)
+    ou, ov = oracle.gen_er(20000, 100000, 0)
+    assert np.array_equal(_np(du), ou) and np.array_equal(_np(dv), ov)
+    du, dv = core.gen_lattice(100, 120, 0.3, 0.05, seed=0, device=dev)
+    ou, ov = oracle.gen_lattice(100, 120, 0.3, 0.05, 0)
+    assert np.array_equal(_np(du), ou) and np.array_equal(_np(dv), ov)
+    cum = oracle.chung_lu_table(5000, 2.1)
+    du, dv = core.gen_chung_lu(5000, 12, 2.1, seed=3, device=dev, cum=cum)
+    ou, ov = oracle.gen_chung_lu(5000, 12, 2.1, 3)
+    assert np.array_equal(_np(du), ou) and np.array_equal(_np(dv), ov)
+
+
+# ------------------------------------------------------------- CSR + exact
+@pytest.mark.parametrize("gname", ["k4_tail", "er_2000", "rmat10", "rmat12", "lattice_40"])
+def test_golden_graphs_exact(tchll, oracle, golden, dev, gname):
+    from triangle_counting_hll_b200 import core
+    from tests.test_oracle_golden import regen
+    arrays, meta = golden
+    case = meta["graphs"][gname]
+    u, v = regen(oracle, gname)
+    g = core.csr_from_edges(u, v, device=dev)
+    _check_csr(g, _ocsr(oracle, u, v))
+    assert _exact(core, g) == case["exact"]
+    # the reference's own GPU entry point signature
+    cnt, elapsed = tchll.gpu_exact_triangle_count(g.row_ptr, g.col_idx, g.edge_u, g.edge_v)
+    assert cnt == case["exact"] and elapsed >= 0.0
+
+
+@pytest.mark.parametrize("scale", [14, 16, 18])
+def test_rmat_exact_vs_oracle(tchll, oracle, dev, scale):
+    from triangle_counting_hll_b200 import core
+    u, v = core.gen_rmat(scale, 16, 0.57, 0.19, 0.19, seed=1, device=dev)
+    g = core.csr_from_edges(u, v)
+    og = _ocsr(oracle, _np(u), _np(v))
+    _check_csr(g, og)
+    ref, pe_ref = oracle.exact_count(og["row_ptr"], og["col_idx"], og["edge_u"], og["edge_v"], nthreads=0,
+                                     per_edge=True)
+    assert _exact(core, g) == ref
+    res, pe = core.exact_count_tensors(g.row_ptr, g.col_idx, g.edge_u, g.edge_v, per_edge=True)
+    assert core.exact_from_result(res) == ref
+    assert np.array_equal(_np(pe), pe_ref)
+
+
+def test_c1_c2_configs(tchll, oracle, dev):
+    """Erdos-Renyi n=20000 m=100000 seed 0 and the 1000x1000 perturbed lattice."""
+    from triangle_counting_hll_b200 import core
+    for u, v in (core.gen_er(20000, 100000, seed=0, device=dev), core.gen_lattice(1000, 1000, 0.3, 0.05, 0, dev)):
+        g = core.csr_from_edges(u, v)
+        og = _ocsr(oracle, _np(u), _np(v))
+        _check_csr(g, og)
+        assert _exact(core, g) == oracle.exact_count(og["row_ptr"], og["col_idx"], og["edge_u"], og["edge_v"])
+
+
+def test_known_answers_and_edge_cases(tchll, dev):
+    from triangle_counting_hll_b200 import core
+    import torch
+    # K_n: C(n,3); n=1200 puts rows above the warp-table capacity (fallback path)
+    for n in (3, 5, 40, 300, 1200, 2500):
+        iu, iv = np.triu_indices(n, 1)
+        g = core.csr_from_edges(iu.astype(np.int32), iv.astype(np.int32), device=dev)
+        assert _exact(core, g) == n * (n - 1) * (n - 2) // 6, n
+    # star, bipartite, single edge, self-loops only, duplicates
+    g = core.csr_from_edges(np.zeros(5000, np.int32), np.arange(1, 5001, dtype=np.int32), device=dev)
+    assert _exact(core, g) == 0 and g.n_edges == 5000
+    a, b = np.meshgrid(np.arange(50), np.arange(50, 120))
+    g = core.csr_from_edges(a.ravel().astype(np.int32), b.ravel().astype(np.int32), device=dev)
+    assert _exact(core, g) == 0
+    g = core.csr_from_edges(np.array([7], np.int32), np.array([3], np.int32), device=dev)
+    assert g.n_nodes == 2 and g.n_edges == 1 and _exact(core, g) == 0
+    g = core.csr_from_edges(np.array([1, 2, 2], np.int32), np.array([1, 2, 2], np.int32), device=dev)
+    assert g.n_nodes == 0 and g.n_edges == 0 and _exact(core, g) == 0
+    tri = np.array([[0, 1], [1, 2], [2, 0], [1, 0], [0, 2], [2, 1], [0, 1]], np.int32)
+    g = core.csr_from_edges(tri[:, 0], tri[:, 1], device=dev)
+    assert g.n_edges == 3 and _exact(core, g) == 1
+    # empty edge list
+    g = core.csr_from_edges(np.zeros(0, np.int32), np.zeros(0, np.int32), device=dev)
+    assert g.n_nodes == 0 and _exact(core, g) == 0
+    # empty edge subset of a real graph
+    g = core.csr_from_edges(np.array([0, 1, 2], np.int32), np.array([1, 2, 0], np.int32), device=dev)
+    e = torch.zeros(0, dtype=torch.int32, device=dev)
+    res, _ = core.exact_count_tensors(g.row_ptr, g.col_idx, e, e)
+    assert core.exact_from_result(res) == 0
+    # negative ids are rejected
+    with pytest.raises(ValueError):
+        core.csr_from_edges(np.array([-1, 2], np.int32), np.array([3, 4], np.int32), device=dev)
+
+
+def test_unsorted_and_subset_edge_lists(tchll, oracle, dev):
+    """The count is a sum over whatever edges are passed, in any order."""
+    from triangle_counting_hll_b200 import core
+    import torch
+    u, v = core.gen_rmat(13, 16, 0.57, 0.19, 0.19, seed=9, device=dev)
+    g = core.csr_from_edges(u, v)
+    og = _ocsr(oracle, _np(u), _np(v))
+    rng = np.random.default_rng(0)
+    perm = rng.permutation(g.n_edges)
+    sub = perm[: g.n_edges // 3]
+    eu = g.edge_u[torch.from_numpy(sub).to(dev)].contiguous()
+    ev = g.edge_v[torch.from_numpy(sub).to(dev)].contiguous()
+    res, _ = core.exact_count_tensors(g.row_ptr, g.col_idx, eu, ev)
+    ref = oracle.exact_count(og["row_ptr"], og["col_idx"], og["edge_u"][sub], og["edge_v"][sub])
+    assert core.exact_from_result(res) == ref
+
+
+def test_malformed_inputs_raise(tchll, dev):
+    from triangle_counting_hll_b200 import core
+    import torch
+    g = core.csr_from_edges(np.array([0, 1, 2], np.int32), np.array([1, 2, 0], np.int32), device=dev)
+    bad = torch.tensor([0, 7], dtype=torch.int32, device=dev)
+    with pytest.raises(ValueError):
+        res, _ = core.exact_count_tensors(g.row_ptr, g.col_idx, bad, bad)
+        core.exact_from_result(res)
+    bad_rp = torch.tensor([0, 5, 1, 3], dtype=torch.int32, device=dev)
+    with pytest.raises(ValueError):
+        res, _ = core.exact_count_tensors(bad_rp, g.col_idx, g.edge_u, g.edge_v)
+        core.exact_from_result(res)
+
+
+def test_tuning_does_not_change_results(tchll, oracle, dev):
+    from triangle_counting_hll_b200 import core
+    u, v = core.gen_rmat(15, 16, 0.57, 0.19, 0.19, seed=2, device=dev)
+    g = core.csr_from_edges(u, v)
+    slot, nr = core.sketch_slots(g.row_ptr, 32)
+    rows = core.build_sketches_compact_tensors(g.row_ptr, g.col_idx, slot, nr, 10)
+    base = core.get_count_tuning()
+    outs = []
+    try:
+        for chunk, lg, tiny in ((64, 11, 16), (32, 8, 0), (256, 12, 64), (1024, 13, 4)):
+            core.set_count_tuning(chunk, lg, tiny, 0)
+            res, _ = core.hybrid_count_compact_tensors(g.row_ptr, g.col_idx, g.edge_u, g.edge_v, g.degrees, rows,
+                                                       slot, 10, 32)
+            tot, r = core.hybrid_from_result(res)
+            outs.append((tot, int(r.exact), int(r.hll_fx_lo), int(r.hll_fx_hi), int(r.n_approx), int(r.n_clamped)))
+            outs.append((_exact(core, g),))
+    finally:
+        core.set_count_tuning(**base)
+    assert len(set(outs[0::2])) == 1 and len(set(outs[1::2])) == 1
+
+
+# ---------------------------------------------------------------- sketches
+@pytest.mark.parametrize("p", [4, 8, 10, 12, 14, 16])
+def test_dense_sketches_bit_exact(tchll, oracle, dev, p):
+    from triangle_counting_hll_b200 import core
+    import torch
+    u, v = core.gen_rmat(12, 16, 0.57, 0.19, 0.19, seed=1, device=dev)
+    g = core.csr_from_edges(u, v)
+    n = g.n_nodes
+    theta = 8
+    og = _ocsr(oracle, _np(u), _np(v))
+    regs = torch.zeros(n << p, dtype=torch.uint8, device=dev)
+    # pre-filled rows are max-merged, as the reference kernel does
+    regs[: 1 << p] = 3
+    has = torch.full((n,), 7, dtype=torch.uint8, device=dev)
+    tchll.build_sketches_kernel[(n + 255) // 256, 256](g.row_ptr, g.col_idx, n, theta, p, regs, has)
+    oregs = np.zeros(n << p, np.uint8)
+    oregs[: 1 << p] = 3
+    oregs, ohas = oracle.build_sketches_dense(og["row_ptr"], og["col_idx"], n, theta, p, oregs)
+    assert np.array_equal(_np(has), ohas)
+    assert np.array_equal(_np(regs), oregs)
+
+
+def test_dense_sketch_launch_covers_grid_only(tchll, oracle, dev):
+    """Like the Numba launch, only u < grid*block are processed."""
+    from triangle_counting_hll_b200 import core
+    import torch
+    u, v = core.gen_rmat(10, 16, 0.57, 0.19, 0.19, seed=1, device=dev)
+    g = core.csr_from_edges(u, v)
+    n, p = g.n_nodes, 8
+    regs = torch.zeros(n << p, dtype=torch.uint8, device=dev)
+    has = torch.full((n,), 9, dtype=torch.uint8, device=dev)
+    tchll.build_sketches_kernel[1, 100](g.row_ptr, g.col_idx, n, 4, p, regs, has)
+    h = _np(has)
+    assert set(h[:100].tolist()) <= {0, 1} and (h[100:] == 9).all()
+
+
+@pytest.mark.parametrize("p", [4, 9, 12, 16])
+def test_compact_sketches_bit_exact(tchll, oracle, dev, p):
+    from triangle_counting_hll_b200 import core
+    u, v = core.gen_rmat(13, 16, 0.57, 0.19, 0.19, seed=4, device=dev)
+    g = core.csr_from_edges(u, v)
+    og = _ocsr(oracle, _np(u), _np(v))
+    slot, nr = core.sketch_slots(g.row_ptr, 16)
+    rows = core.build_sketches_compact_tensors(g.row_ptr, g.col_idx, slot, nr, p)
+    oslot, orows = oracle.build_sketches_compact(og["row_ptr"].astype(np.int64), og["col_idx"].astype(np.int64),
+                                                 16, p)
+    assert np.array_equal(_np(slot), oslot) and nr == int((oslot >= 0).sum())
+    assert np.array_equal(_np(rows), orows)
+    # hashing a per-node key table (original ids)
+    keys = g.node_ids.to(dtype=__import__("torch").int64) * 1000003 + 11
+    rows2 = core.build_sketches_compact_tensors(g.row_ptr, g.col_idx, slot, nr, p, keys=keys)
+    kh = _np(keys)
+    _, orows2 = oracle.build_sketches_compact(og["row_ptr"].astype(np.int64), kh[og["col_idx"]], 16, p)
+    assert np.array_equal(_np(rows2), orows2)
+
+
+# ------------------------------------------------------------------- HLL
+@pytest.mark.parametrize("p", list(range(4, 17)))
+def test_hll_class_vs_golden(tchll, golden, p):
+    arrays, meta = golden
+    for name in ("ids_0_100", "ids_0_5000", "rand_300", "rand_20000", "single_0"):
+        h = tchll.HLL(p=p)
+        h.add_array(arrays[f"set_{name}"])
+        assert np.array_equal(h.registers, arrays[f"regs_{name}_p{p}"]), (name, p)
+        assert h.estimate() == pytest.approx(meta["estimates"][f"{name}_p{p}"], rel=EST_RTOL)
+        assert h.memory_bytes() == 1 << p
+
+
+def test_hll_add_scalars_and_union(tchll, golden):
+    from triangle_counting_hll_b200 import hll as H
+    arrays, meta = golden
+    h = tchll.HLL(p=8)
+    for x in arrays["set_rand_300"][:150]:
+        h.add(int(x))
+    h.add_array(arrays["set_rand_300"][150:])
+    assert np.array_equal(h.registers, arrays["regs_rand_300_p8"])
+    for key, ref in meta["unions"].items():
+        p = int(key.split("_")[0][1:])
+        a, b = tchll.HLL(p=p), tchll.HLL(p=p)
+        a.registers = arrays[f"ua_{key}"]
+        b.registers = arrays[f"ub_{key}"]
+        assert tchll.union_estimate(a, b) == pytest.approx(ref, rel=EST_RTOL), key
+    with pytest.raises(ValueError):
+        tchll.union_estimate(tchll.HLL(p=8), tchll.HLL(p=10))
+    with pytest.raises(ValueError):
+        tchll.HLL(p=3)
+    with pytest.raises(ValueError):
+        tchll.HLL(p=17)
+    assert H._hash64(0) == 0
+    hv = H.hash64_array(arrays["hash_in"])
+    assert np.array_equal(hv, arrays["hash_out"])
+
+
+# ----------------------------------------------------------------- hybrid
+@pytest.mark.parametrize("gname", ["er_2000", "rmat10", "rmat12", "lattice_40"])
+def test_hybrid_vs_golden(tchll, oracle, golden, dev, gname):
+    from triangle_counting_hll_b200 import core
+    from tests.test_oracle_golden import regen
+    arrays, meta = golden
+    case = meta["graphs"][gname]
+    u, v = regen(oracle, gname)
+    g = core.csr_from_edges(u, v, device=dev)
+    for theta, p in ((8, 8), (16, 10), (32, 12), (4, 4)):
+        key = f"t{theta}_p{p}"
+        for suffix, th in (("", theta), ("_fallback", 2 * theta)):
+            slot, nr = core.sketch_slots(g.row_ptr, th)
+            rows = core.build_sketches_compact_tensors(g.row_ptr, g.col_idx, slot, nr, p)
+            for split in (False, True):
+                res, pe = core.hybrid_count_compact_tensors(g.row_ptr, g.col_idx, g.edge_u, g.edge_v, g.degrees,
+                                                            rows, slot, p, theta, split_kernels=split,
+                                                            details=(suffix == ""))
+                tot, r = core.hybrid_from_result(res)
+                ref = case["hybrid"][key + suffix]
+                assert tot == pytest.approx(ref["total"], rel=HYB_RTOL), (key + suffix, split)
+                st = ref["stats"]
+                assert (int(r.n_approx), int(r.n_fallback), int(r.n_clamped)) == \
+                    (st["n_approx"], st["n_fallback"], st["n_clamped"]), (key + suffix, split)
+                assert int(r.n_approx) + int(r.n_exact) == st["n_edges"]
+                if pe is not None and f"g_{gname}_{key}_s_hat" in arrays:
+                    method = _np(pe[3])
+                    assert np.array_equal(method, arrays[f"g_{gname}_{key}_method"])
+                    s = np.where(method == 1, _np(pe[1]), _np(pe[0]).astype(np.float64))
+                    np.testing.assert_allclose(s, arrays[f"g_{gname}_{key}_s_hat"], rtol=EST_RTOL, atol=1e-9)
+
+
+@pytest.mark.parametrize("p", [8, 10, 12, 14])
+def test_hybrid_dense_rmat_vs_oracle(tchll, oracle, dev, p):
+    """The reference GPU entry point (dense registers, theta = gamma)."""
+    from triangle_counting_hll_b200 import core
+    import torch
+    u, v = core.gen_rmat(16, 16, 0.57, 0.19, 0.19, seed=1, device=dev)
+    g = core.csr_from_edges(u, v)
+    n, gamma = g.n_nodes, 64
+    regs, has = tchll.alloc_sketch_arrays_device(n, p)
+    tchll.build_sketches_kernel[(n + 255) // 256, 256](g.row_ptr, g.col_idx, n, gamma, p, regs, has)
+    og = _ocsr(oracle, _np(u), _np(v))
+    oregs, ohas = oracle.build_sketches_dense(og["row_ptr"], og["col_idx"], n, gamma, p)
+    assert np.array_equal(_np(regs), oregs)
+    otot, ost, _ = oracle.hybrid_count(og["row_ptr"], og["col_idx"], og["edge_u"], og["edge_v"], og["degrees"],
+                                       oracle.dense_slots(ohas), oregs, p, gamma, nthreads=0)
+    for split in (True, False):
+        est, el, st = tchll.gpu_hybrid_triangle_count(g.row_ptr, g.col_idx, g.edge_u, g.edge_v, g.degrees, regs, has,
+                                                      gamma, p, split_kernels=split)
+        assert est == pytest.approx(otot, rel=HYB_RTOL)
+        assert st["n_approx"] == ost["n_approx"] and st["n_clamped"] == ost["n_clamped"]
+        assert st["n_exact"] == ost["n_exact"]
+        assert st["kernel_mode"] == ("split_block_reduction" if split else "fused_block_reduction")
+
+
+def test_hybrid_all_exact_equals_exact(tchll, dev):
+    """gamma above every forward degree: hybrid == exact (configs C1/C2)."""
+    from triangle_counting_hll_b200 import core
+    for u, v in (core.gen_er(20000, 100000, seed=0, device=dev), core.gen_lattice(300, 300, 0.3, 0.05, 0, dev)):
+        g = core.csr_from_edges(u, v)
+        slot, nr = core.sketch_slots(g.row_ptr, 16)
+        rows = core.build_sketches_compact_tensors(g.row_ptr, g.col_idx, slot, nr, 10)
+        res, _ = core.hybrid_count_compact_tensors(g.row_ptr, g.col_idx, g.edge_u, g.edge_v, g.degrees, rows, slot,
+                                                   10, 16)
+        tot, r = core.hybrid_from_result(res)
+        assert tot == float(_exact(core, g)) and int(r.n_approx) == 0
+
+
+# ------------------------------------------------- forward_adj drop-in API
+@pytest.mark.parametrize("gname", ["k4_tail", "er_2000", "rmat10", "lattice_40"])
+def test_cpu_path_api_vs_golden(tchll, oracle, golden, gname):
+    from tests.test_oracle_golden import regen
+    arrays, meta = golden
+    case = meta["graphs"][gname]
+    u, v = regen(oracle, gname)
+    edges = {(min(a, b), max(a, b)) for a, b in zip(u.tolist(), v.tolist()) if a != b}
+    fwd, degree = tchll.orient_graph(edges)
+    assert np.array_equal(np.array([degree[k] for k in sorted(degree)]), arrays[f"g_{gname}_undeg"])
+    cnt, el, ed = tchll.exact_triangle_count(fwd)
+    assert cnt == case["exact"]
+    cnt2, _, recs = tchll.exact_triangle_count(fwd, per_edge_timing=True)
+    assert cnt2 == cnt and sum(r[4] for r in recs) == cnt
+    rp, ci, dg, ids, eu, ev = tchll.to_csr_numpy(fwd)
+    if f"g_{gname}_row_ptr" in arrays:
+        for nm, a in (("row_ptr", rp), ("col_idx", ci), ("degrees", dg), ("node_ids", ids), ("edge_u", eu),
+                      ("edge_v", ev)):
+            assert np.array_equal(a, arrays[f"g_{gname}_{nm}"]), nm
+    # original-id sketches (src/hybrid.py:39)
+    sk = tchll.build_sketches(fwd, 8, 8)
+    if f"g_{gname}_origsk_keys" in arrays:
+        keys = arrays[f"g_{gname}_origsk_keys"]
+        assert sorted(sk) == keys.tolist()
+        got = np.stack([sk[int(k)].registers for k in keys])
+        assert np.array_equal(got, arrays[f"g_{gname}_origsk_regs"])
+    tot, el, st, det = tchll.hybrid_triangle_count(fwd, sk, 8, record_details=True)
+    ref = case["hybrid"]["orig_ids_t8_p8"]
+    assert tot == pytest.approx(ref["total"], rel=HYB_RTOL)
+    for k in ("n_edges", "n_approx", "n_exact", "n_fallback", "n_clamped"):
+        assert st[k] == ref["stats"][k], k
+    assert len(det) == st["n_edges"]
+    assert sum(d["s_clamped"] for d in det) == pytest.approx(tot, rel=1e-9)
+
+
+def test_intersect_helpers(tchll):
+    a = np.array([1, 3, 5, 7, 9, 11], dtype=np.int64)
+    b = np.array([3, 4, 5, 11, 20], dtype=np.int64)
+    assert tchll.intersect_merge(a, b) == 3
+    assert tchll.intersect_bsearch(np.array([5, 11]), b) == 2
+    assert tchll.intersect_adaptive(a, b) == 3
+    assert tchll.intersect_adaptive(np.array([], dtype=np.int64), b) == 0
+
+
+# ------------------------------------------------------------------ ingest
+def test_device_edge_text_parse(tchll, tmp_path):
+    from triangle_counting_hll_b200 import ingest
+    text = ("# comment\n% other comment\n\n  1 2\n3\t4 extra tokens\n5 5\n6\n"
+            "  # indented comment\n-7 8\r\n9 10")
+    u, v = ingest.parse_edge_text(text.encode())
+    assert _np(u).tolist() == [1, 3, 5, -7, 9] and _np(v).tolist() == [2, 4, 5, 8, 10]
+    p = tmp_path / "g.txt"
+    p.write_text("# snap header\n0 1\n1 2\n2 0\n2 3\n3 3\n1 0\n")
+    assert tchll.load_edgelist(str(p)) == {(0, 1), (1, 2), (0, 2), (2, 3)}
+    with pytest.raises(ValueError):
+        ingest.parse_edge_text(b"1 x\n")
+    g = ingest.load_graph(str(p))
+    assert g.n_edges == 4 and g.n_nodes == 4

@@ -1,0 +1,550 @@
+// count.cu -- exact and hybrid (exact / HyperLogLog) triangle counting.
+//
+// Reference semantics (ChitandaEruQ/triangle_counting_hll):
+//   exact:   T = sum over oriented edges (u,v) of |N+(u) cap N+(v)|
+//            src/exact.py:48-98, src/gpu_hybrid.py:96-130,332-354
+//   hybrid:  edge -> HLL iff min(d+u, d+v) >= gamma and both endpoints carry a
+//            sketch (src/hybrid.py:107-115, src/gpu_hybrid.py:80-89); HLL edges
+//            add clamp(d+u + d+v - |N+(u) cup N+(v)|^, 0, min(d+u, d+v))
+//            (src/hybrid.py:117-126, src/gpu_hybrid.py:288-302), the union
+//            estimated from the register-wise max of the two sketches with the
+//            reference's bias and range corrections (src/hll.py:37-54,112-120).
+//
+// Design (one persistent launch, work stealing over edge chunks):
+//   * A warp claims CHUNK consecutive edges with one atomicAdd and walks them
+//     32 at a time.  Within a batch, edges that share u form a group; the warp
+//     keeps N+(u) in a private shared-memory hash table (open addressing,
+//     load <= 1/4 where the capacity allows) that survives across groups and
+//     batches while u does not change, so a CSR-ordered edge list builds each
+//     row's table about once per chunk.
+//   * The group's probe lists N+(v) are flattened into one stream of 16-byte
+//     quads and dealt to the 32 lanes with a warp scan, so short and long
+//     lists keep every lane busy.  Each element costs one hash probe.
+//   * Edges whose two lists are both tiny are merged lane-locally; rows too
+//     long for a warp table fall back to a warp binary search.
+//   * HLL edges: the warp reads both 2^p-byte register rows with 16-byte loads,
+//     merges them with __vmaxu4 and accumulates sum 2^-r EXACTLY as a 128-bit
+//     fixed-point integer (zero registers counted with __vcmpeq4), then one
+//     lane applies alpha*m^2/Z, linear counting and the 2^64 correction in
+//     FP64, clamps, and adds the result in 2^-32 fixed point.
+//   * All totals are integers (uint64 exact count, 128-bit fixed-point HLL sum,
+//     int64 stats) added with integer atomics, so results do not depend on
+//     scheduling: any partition of the edges gives bit-identical totals.
+#include "common.cuh"
+#include "hll_device.cuh"
+
+namespace tchll {
+
+enum : int { MODE_EXACT = 0, MODE_HYBRID = 1, MODE_HYB_EXACT = 2, MODE_HYB_HLL = 3 };
+
+enum : uint32_t {
+    ST_BAD_EDGE = 1u,   // edge endpoint outside [0, n_nodes)
+    ST_BAD_ROW = 2u,    // row_ptr extent outside [0, nnz] or decreasing
+    ST_BAD_SLOT = 4u,   // sketch slot outside [0, n_rows)
+};
+
+struct CountParams {
+    const int32_t* row_ptr;
+    int64_t n_nodes;
+    const int32_t* col_idx;
+    int64_t nnz;
+    const int32_t* edge_u;
+    const int32_t* edge_v;
+    int64_t n_edges;
+    const int32_t* degrees;  // forward degree for routing (hybrid modes)
+    const uint8_t* regs;     // register rows
+    int64_t n_rows;          // rows available in regs
+    const int64_t* slot;     // compact layout: row of v, or -1; null -> dense
+    const uint8_t* has;      // dense layout: has_sketch[v] == 1 -> row v
+    int p;
+    int64_t gamma;
+    int64_t* pe_support;     // per-edge exact support (details), zeroed by host
+    double* pe_s_hat;        // per-edge HLL s_hat (details)
+    double* pe_s_cl;         // per-edge HLL clamped support (details)
+    uint8_t* pe_method;      // per-edge 0 exact / 1 hll (details)
+    tchll_count_result* result;
+    unsigned long long* work;
+    int chunk;
+    int slots_log2;          // per-warp table capacity (log2 slots)
+    int tiny;                // lane-local merge when |N+u| + |N+v| <= tiny
+};
+
+__device__ __forceinline__ uint32_t tbl_hash(int32_t x, int lg) {
+    return ((uint32_t)x * 0x9E3779B1u) >> (32 - lg);
+}
+
+__device__ __forceinline__ int tbl_probe(const int32_t* table, int lg, int32_t x) {
+    const uint32_t mask = (1u << lg) - 1u;
+    uint32_t h = tbl_hash(x, lg);
+    while (true) {
+        int32_t y = table[h];
+        if (y == x) return 1;
+        if (y < 0) return 0;
+        h = (h + 1u) & mask;
+    }
+}
+
+__device__ __forceinline__ int ceil_log2_i(int x) { return x <= 1 ? 0 : 32 - __clz(x - 1); }
+
+// Warp-cooperative binary-search intersection count of two sorted lists in
+// global memory (used for rows too long for a warp table).  Returns per-lane
+// partial counts.
+__device__ __forceinline__ uint32_t warp_bsearch_count(const int32_t* a, int la, const int32_t* b, int lb,
+                                                       int lane) {
+    if (la > lb) { const int32_t* t = a; a = b; b = t; int tl = la; la = lb; lb = tl; }
+    uint32_t c = 0;
+    for (int i = lane; i < la; i += 32) {
+        int32_t x = __ldg(a + i);
+        int lo = 0, hi = lb;
+        while (lo < hi) {
+            int mid = (lo + hi) >> 1;
+            if (__ldg(b + mid) < x) lo = mid + 1; else hi = mid;
+        }
+        c += (lo < lb && __ldg(b + lo) == x);
+    }
+    return c;
+}
+
+__device__ __forceinline__ uint32_t lane_merge_count(const int32_t* a, int la, const int32_t* b, int lb) {
+    int i = 0, j = 0;
+    uint32_t c = 0;
+    while (i < la && j < lb) {
+        int32_t x = __ldg(a + i), y = __ldg(b + j);
+        c += (x == y);
+        i += (x <= y);
+        j += (y <= x);
+    }
+    return c;
+}
+
+template <int MODE, bool VEC, bool DETAILS>
+__global__ void __launch_bounds__(256, 1) count_kernel(const CountParams P) {
+    extern __shared__ __align__(16) int32_t smem[];
+    const int lane = threadIdx.x & 31;
+    const int wid = threadIdx.x >> 5;
+    const int cap_lg = P.slots_log2;
+    const int cap_keys = 1 << (cap_lg - 1);
+    int32_t* table = smem + ((size_t)wid << cap_lg);
+
+    const int32_t* __restrict__ row_ptr = P.row_ptr;
+    const int32_t* __restrict__ col_idx = P.col_idx;
+
+    uint64_t acc = 0;
+    U128 hacc;
+    int64_t n_approx = 0, n_exact = 0, n_fallback = 0, n_clamped = 0;
+    uint32_t status = 0;
+    int cur_u = -1;
+    int cur_lg = 5;
+    const int m = 1 << P.p;
+
+    while (true) {
+        unsigned long long e0 = 0;
+        if (lane == 0) e0 = atomicAdd(P.work, (unsigned long long)P.chunk);
+        e0 = __shfl_sync(FULL, e0, 0);
+        if (e0 >= (unsigned long long)P.n_edges) break;
+        const int64_t e1 = min((int64_t)e0 + P.chunk, P.n_edges);
+        for (int64_t eb = (int64_t)e0; eb < e1; eb += 32) {
+            const int64_t e = eb + lane;
+            bool valid = e < e1;
+            int32_t u = 0, v = 0, us = 0, ue = 0, vs = 0, ve = 0;
+            if (valid) {
+                u = __ldg(P.edge_u + e);
+                v = __ldg(P.edge_v + e);
+                if ((uint64_t)(uint32_t)u >= (uint64_t)P.n_nodes || (uint64_t)(uint32_t)v >= (uint64_t)P.n_nodes ||
+                    u < 0 || v < 0) {
+                    status |= ST_BAD_EDGE;
+                    valid = false;
+                }
+            }
+            if (valid) {
+                us = __ldg(row_ptr + u); ue = __ldg(row_ptr + u + 1);
+                vs = __ldg(row_ptr + v); ve = __ldg(row_ptr + v + 1);
+                if (us < 0 || ue < us || (int64_t)ue > P.nnz || vs < 0 || ve < vs || (int64_t)ve > P.nnz) {
+                    status |= ST_BAD_ROW;
+                    valid = false;
+                }
+            }
+            bool is_hll = false;
+            int64_t slot_u = -1, slot_v = -1;
+            int32_t du = 0, dv = 0;
+            if (MODE != MODE_EXACT && valid) {
+                du = __ldg(P.degrees + u);
+                dv = __ldg(P.degrees + v);
+                const int64_t proxy = du < dv ? du : dv;
+                const bool wants = proxy >= P.gamma;
+                if (P.slot) {
+                    slot_u = __ldg(P.slot + u);
+                    slot_v = __ldg(P.slot + v);
+                } else {
+                    slot_u = __ldg(P.has + u) == 1 ? (int64_t)u : -1;
+                    slot_v = __ldg(P.has + v) == 1 ? (int64_t)v : -1;
+                }
+                if (slot_u >= P.n_rows || slot_v >= P.n_rows) { status |= ST_BAD_SLOT; valid = false; }
+                const bool both = slot_u >= 0 && slot_v >= 0;
+                is_hll = valid && wants && both;
+                if (MODE != MODE_HYB_HLL && valid && wants && !both) ++n_fallback;
+            }
+            const bool do_exact = valid && !is_hll && MODE != MODE_HYB_HLL;
+            const bool do_hll = valid && is_hll && MODE != MODE_HYB_EXACT;
+            n_exact += do_exact;
+
+            // ---------------------------------------------------- exact part
+            const int lu = ue - us, lv = ve - vs;
+            const bool tiny = do_exact && (lu + lv <= P.tiny || lu == 0 || lv == 0);
+            if (tiny) {
+                uint32_t c = (lu && lv) ? lane_merge_count(col_idx + us, lu, col_idx + vs, lv) : 0u;
+                acc += c;
+                if (DETAILS) P.pe_support[e] = c;
+            }
+            unsigned pend = __ballot_sync(FULL, do_exact && !tiny);
+            while (pend) {
+                const int lead = __ffs(pend) - 1;
+                const int32_t ucur = __shfl_sync(FULL, u, lead);
+                const unsigned grp = __ballot_sync(FULL, ((pend >> lane) & 1u) && u == ucur);
+                pend &= ~grp;
+                const int32_t gus = __shfl_sync(FULL, us, lead);
+                const int32_t gdu = __shfl_sync(FULL, lu, lead);
+                const bool in = (grp >> lane) & 1u;
+                if (gdu > cap_keys) {
+                    // row too long for a warp table: binary search per edge
+                    unsigned g = grp;
+                    while (g) {
+                        const int j = __ffs(g) - 1;
+                        g &= g - 1;
+                        const int32_t jvs = __shfl_sync(FULL, vs, j);
+                        const int32_t jlv = __shfl_sync(FULL, lv, j);
+                        uint32_t c = warp_bsearch_count(col_idx + gus, gdu, col_idx + jvs, jlv, lane);
+                        acc += c;
+                        if (DETAILS) {
+                            uint32_t tot = (uint32_t)warp_sum_u64(c);
+                            const int64_t ej = __shfl_sync(FULL, e, j);
+                            if (lane == 0) P.pe_support[ej] = tot;
+                        }
+                    }
+                    continue;
+                }
+                if (ucur != cur_u) {
+                    // (re)build the warp's table for N+(ucur)
+                    int lg = ceil_log2_i(gdu) + 2;
+                    lg = lg < 5 ? 5 : (lg > cap_lg ? cap_lg : lg);
+                    const int sz = 1 << lg;
+                    __syncwarp();
+                    for (int i = lane; i < sz; i += 32) table[i] = -1;
+                    __syncwarp();
+                    const uint32_t mask = (uint32_t)sz - 1u;
+                    for (int i = lane; i < gdu; i += 32) {
+                        const int32_t x = __ldg(col_idx + gus + i);
+                        uint32_t h = tbl_hash(x, lg);
+                        while (true) {
+                            const int32_t old = atomicCAS(&table[h], -1, x);
+                            if (old == -1 || old == x) break;
+                            h = (h + 1u) & mask;
+                        }
+                    }
+                    __syncwarp();
+                    cur_u = ucur;
+                    cur_lg = lg;
+                }
+                // flatten the group's probe lists N+(v) into quads
+                int q0, nq;
+                if (VEC) {
+                    q0 = vs >> 2;
+                    nq = (in && ve > vs) ? ((ve - 1) >> 2) - q0 + 1 : 0;
+                } else {
+                    q0 = vs;
+                    nq = in ? (ve - vs) : 0;
+                }
+                const unsigned ne = __ballot_sync(FULL, nq > 0);
+                const int k = __popc(ne);
+                const int src = lane < k ? (int)__fns(ne, 0, lane + 1) : lane;
+                const int c_q0 = __shfl_sync(FULL, q0, src);
+                int c_nq = __shfl_sync(FULL, nq, src);
+                const int32_t c_vs = __shfl_sync(FULL, vs, src);
+                const int32_t c_ve = __shfl_sync(FULL, ve, src);
+                int64_t c_e = 0;
+                if (DETAILS) c_e = __shfl_sync(FULL, e, src);
+                if (lane >= k) c_nq = 0;
+                int incl = c_nq;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(FULL, incl, o);
+                    if (lane >= o) incl += t;
+                }
+                const int excl = incl - c_nq;
+                const int W = __shfl_sync(FULL, incl, 31);
+                const int qb = c_q0 - excl;
+                for (int T0 = 0; T0 < W; T0 += 32) {
+                    const unsigned cover = __ballot_sync(FULL, lane < k && excl <= T0 && T0 < incl);
+                    const int b = __ffs(cover) - 1;
+                    const unsigned bit = (lane < k && excl > T0 && excl < T0 + 32) ? (1u << (excl - T0)) : 0u;
+                    const unsigned B = __reduce_or_sync(FULL, bit);
+                    const int j = (b + __popc(B & ((2u << lane) - 1u))) & 31;
+                    const int my_qb = __shfl_sync(FULL, qb, j);
+                    const int32_t my_vs = __shfl_sync(FULL, c_vs, j);
+                    const int32_t my_ve = __shfl_sync(FULL, c_ve, j);
+                    int64_t my_e = 0;
+                    if (DETAILS) my_e = __shfl_sync(FULL, c_e, j);
+                    const int t = T0 + lane;
+                    if (t < W) {
+                        const int qd = my_qb + t;
+                        uint32_t c = 0;
+                        if (VEC) {
+                            const int base = qd * 4;
+                            int4 val;
+                            if ((int64_t)base + 3 < P.nnz) {
+                                val = __ldg(reinterpret_cast<const int4*>(col_idx) + qd);
+                            } else {
+                                val.x = base + 0 < P.nnz ? __ldg(col_idx + base + 0) : -1;
+                                val.y = base + 1 < P.nnz ? __ldg(col_idx + base + 1) : -1;
+                                val.z = base + 2 < P.nnz ? __ldg(col_idx + base + 2) : -1;
+                                val.w = base + 3 < P.nnz ? __ldg(col_idx + base + 3) : -1;
+                            }
+                            if (base + 0 >= my_vs && base + 0 < my_ve) c += tbl_probe(table, cur_lg, val.x);
+                            if (base + 1 >= my_vs && base + 1 < my_ve) c += tbl_probe(table, cur_lg, val.y);
+                            if (base + 2 >= my_vs && base + 2 < my_ve) c += tbl_probe(table, cur_lg, val.z);
+                            if (base + 3 >= my_vs && base + 3 < my_ve) c += tbl_probe(table, cur_lg, val.w);
+                        } else {
+                            c = tbl_probe(table, cur_lg, __ldg(col_idx + qd));
+                        }
+                        acc += c;
+                        if (DETAILS && c) atomicAdd((unsigned long long*)(P.pe_support + my_e), (unsigned long long)c);
+                    }
+                }
+            }
+
+            // ------------------------------------------------------ HLL part
+            if (MODE != MODE_EXACT && MODE != MODE_HYB_EXACT) {
+                unsigned hm = __ballot_sync(FULL, do_hll);
+                while (hm) {
+                    const int j = __ffs(hm) - 1;
+                    hm &= hm - 1;
+                    const int64_t su = __shfl_sync(FULL, slot_u, j);
+                    const int64_t sv = __shfl_sync(FULL, slot_v, j);
+                    const int32_t jdu = __shfl_sync(FULL, du, j);
+                    const int32_t jdv = __shfl_sync(FULL, dv, j);
+                    const uint8_t* ra = P.regs + su * (int64_t)m;
+                    const uint8_t* rb = P.regs + sv * (int64_t)m;
+                    const double E = warp_union_estimate<VEC>(ra, rb, P.p, lane);
+                    if (lane == 0) {
+                        const double s_hat = (double)((int64_t)jdu + (int64_t)jdv) - E;
+                        const double upper = (double)(jdu < jdv ? jdu : jdv);
+                        // max(0.0, min(s_hat, upper)) with Python's min/max
+                        // argument order (src/hybrid.py:122)
+                        double s_cl = (upper < s_hat) ? upper : s_hat;
+                        s_cl = (s_cl > 0.0) ? s_cl : 0.0;
+                        if (s_hat < 0.0 || s_hat > upper) ++n_clamped;
+                        ++n_approx;
+                        hacc.add((uint64_t)__double2ull_rn(s_cl * 4294967296.0));
+                        if (DETAILS) {
+                            const int64_t ej = eb + j;
+                            P.pe_s_hat[ej] = s_hat;
+                            P.pe_s_cl[ej] = s_cl;
+                            P.pe_method[ej] = 1;
+                        }
+                    }
+                }
+            }
+        }
+    }
+
+    // ---------------------------------------------------------- publish ----
+    acc = warp_sum_u64(acc);
+    n_approx = warp_sum_i64(n_approx);
+    n_exact = warp_sum_i64(n_exact);
+    n_fallback = warp_sum_i64(n_fallback);
+    n_clamped = warp_sum_i64(n_clamped);
+    status = __reduce_or_sync(FULL, status);
+    if (lane == 0) {
+        tchll_count_result* R = P.result;
+        if (acc) atomicAdd((unsigned long long*)&R->exact, (unsigned long long)acc);
+        atomic_add_u128((unsigned long long*)&R->hll_fx_lo, hacc);
+        if (n_approx) atomicAdd((unsigned long long*)&R->n_approx, (unsigned long long)n_approx);
+        if (n_exact) atomicAdd((unsigned long long*)&R->n_exact, (unsigned long long)n_exact);
+        if (n_fallback) atomicAdd((unsigned long long*)&R->n_fallback, (unsigned long long)n_fallback);
+        if (n_clamped) atomicAdd((unsigned long long*)&R->n_clamped, (unsigned long long)n_clamped);
+        if (status) atomicOr(&R->status, status);
+    }
+}
+
+// ---------------------------------------------------------------- host ------
+static constexpr int kWarps = 8;
+static constexpr int kThreads = kWarps * 32;
+
+struct Tuning {
+    int chunk = 64;
+    int slots_log2 = 11;  // 2048 slots = 8 KB per warp
+    int tiny = 16;
+    int blocks_per_sm = 0;  // 0: occupancy maximum
+};
+static Tuning g_tuning;
+
+template <int MODE, bool VEC, bool DETAILS>
+static int launch_mode(const CountParams& P, cudaStream_t st) {
+    auto kern = count_kernel<MODE, VEC, DETAILS>;
+    const size_t smem = (size_t)kWarps * ((size_t)1 << P.slots_log2) * sizeof(int32_t);
+    static size_t smem_set = 0;  // largest dynamic smem opted into so far
+    cudaError_t e;
+    if (smem > smem_set) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(count_kernel)");
+        smem_set = smem;
+    }
+    int bps = g_tuning.blocks_per_sm;
+    if (bps <= 0) {
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, kThreads, smem);
+        if (e != cudaSuccess) return cuda_status(e, "occupancy(count_kernel)");
+        if (bps < 1) bps = 1;
+    }
+    const int grid = sm_count() * bps;
+    kern<<<grid, kThreads, smem, st>>>(P);
+    TCHLL_CHECK_LAUNCH("count_kernel");
+    return TCHLL_OK;
+}
+
+template <int MODE>
+static int launch_count(const CountParams& P, bool details, cudaStream_t st) {
+    const bool vec = ((uintptr_t)P.col_idx % 16 == 0) && (P.regs == nullptr || (uintptr_t)P.regs % 16 == 0);
+    if (details) return vec ? launch_mode<MODE, true, true>(P, st) : launch_mode<MODE, false, true>(P, st);
+    return vec ? launch_mode<MODE, true, false>(P, st) : launch_mode<MODE, false, false>(P, st);
+}
+
+static int run_count(CountParams P, int mode, bool details, void* ws, size_t ws_bytes, cudaStream_t st) {
+    Carve cv(ws, ws_bytes);
+    unsigned long long* ctr = cv.take<unsigned long long>(2);
+    if (!cv.ok()) { set_error("workspace too small: need %zu bytes, have %zu", cv.off, ws_bytes); return TCHLL_EWORKSPACE; }
+    TCHLL_CUDA(cudaMemsetAsync(ctr, 0, 2 * sizeof(unsigned long long), st));
+    TCHLL_CUDA(cudaMemsetAsync(P.result, 0, sizeof(tchll_count_result), st));
+    if (details && P.pe_support) TCHLL_CUDA(cudaMemsetAsync(P.pe_support, 0, sizeof(int64_t) * P.n_edges, st));
+    if (details && P.pe_method) TCHLL_CUDA(cudaMemsetAsync(P.pe_method, 0, P.n_edges, st));
+    P.chunk = g_tuning.chunk;
+    P.slots_log2 = g_tuning.slots_log2;
+    P.tiny = g_tuning.tiny;
+    if (P.n_edges == 0) return TCHLL_OK;
+    int rc;
+    switch (mode) {
+        case MODE_EXACT:
+            P.work = ctr;
+            return launch_count<MODE_EXACT>(P, details, st);
+        case MODE_HYBRID:
+            P.work = ctr;
+            return launch_count<MODE_HYBRID>(P, details, st);
+        case 2:  // split: exact-routed edges, then HLL-routed edges
+            P.work = ctr;
+            rc = launch_count<MODE_HYB_EXACT>(P, details, st);
+            if (rc) return rc;
+            P.work = ctr + 1;
+            return launch_count<MODE_HYB_HLL>(P, details, st);
+        default:
+            set_error("unknown count mode %d", mode);
+            return TCHLL_EINVAL;
+    }
+}
+
+static int check_common(const int32_t* row_ptr, int64_t n_nodes, const int32_t* col_idx, int64_t nnz,
+                        const int32_t* eu, const int32_t* ev, int64_t n_edges, tchll_count_result* result) {
+    TCHLL_ARG(n_nodes >= 0 && nnz >= 0 && n_edges >= 0, "negative size");
+    TCHLL_ARG(n_nodes < (int64_t)INT32_MAX && nnz <= (int64_t)INT32_MAX, "int32 CSR limits exceeded");
+    TCHLL_ARG(result != nullptr, "result pointer is null");
+    TCHLL_ARG(n_edges == 0 || (eu && ev && row_ptr), "null edge or row_ptr pointer");
+    TCHLL_ARG(nnz == 0 || col_idx, "null col_idx");
+    return TCHLL_OK;
+}
+
+}  // namespace tchll
+
+using namespace tchll;
+
+TCHLL_EXPORT int tchll_count_workspace_bytes(int64_t n_edges, size_t* bytes) {
+    (void)n_edges;
+    if (!bytes) { set_error("bytes is null"); return TCHLL_EINVAL; }
+    Carve cv(nullptr, 0);
+    cv.take<unsigned long long>(2);
+    *bytes = cv.off;
+    return TCHLL_OK;
+}
+
+TCHLL_EXPORT int tchll_exact_count(const int32_t* row_ptr, int64_t n_nodes, const int32_t* col_idx, int64_t nnz,
+                                   const int32_t* edge_u, const int32_t* edge_v, int64_t n_edges,
+                                   int64_t* per_edge_support, tchll_count_result* result, void* workspace,
+                                   size_t workspace_bytes, void* stream) {
+    int rc = check_common(row_ptr, n_nodes, col_idx, nnz, edge_u, edge_v, n_edges, result);
+    if (rc) return rc;
+    CountParams P{};
+    P.row_ptr = row_ptr; P.n_nodes = n_nodes; P.col_idx = col_idx; P.nnz = nnz;
+    P.edge_u = edge_u; P.edge_v = edge_v; P.n_edges = n_edges;
+    P.pe_support = per_edge_support;
+    P.result = result;
+    P.p = 4;
+    return run_count(P, MODE_EXACT, per_edge_support != nullptr, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+static int hybrid_common(const int32_t* row_ptr, int64_t n_nodes, const int32_t* col_idx, int64_t nnz,
+                         const int32_t* edge_u, const int32_t* edge_v, int64_t n_edges, const int32_t* degrees,
+                         const uint8_t* regs, int64_t n_rows, const int64_t* slot, const uint8_t* has, int32_t p,
+                         int64_t gamma, int32_t mode, int64_t* pe_support, double* pe_s_hat, double* pe_s_cl,
+                         uint8_t* pe_method, tchll_count_result* result, void* ws, size_t wsb, void* stream) {
+    int rc = check_common(row_ptr, n_nodes, col_idx, nnz, edge_u, edge_v, n_edges, result);
+    if (rc) return rc;
+    TCHLL_ARG(p >= 4 && p <= 16, "p must be in [4, 16], got %d", p);
+    TCHLL_ARG(mode >= 1 && mode <= 2, "mode must be 1 (fused) or 2 (split), got %d", mode);
+    TCHLL_ARG(n_edges == 0 || degrees, "degrees is null");
+    TCHLL_ARG(n_rows == 0 || regs, "register rows are null");
+    TCHLL_ARG(slot || has || n_edges == 0, "need slot (compact) or has_sketch (dense)");
+    const bool details = pe_support || pe_s_hat || pe_s_cl || pe_method;
+    TCHLL_ARG(!details || (pe_support && pe_s_hat && pe_s_cl && pe_method),
+              "per-edge outputs must be all set or all null");
+    CountParams P{};
+    P.row_ptr = row_ptr; P.n_nodes = n_nodes; P.col_idx = col_idx; P.nnz = nnz;
+    P.edge_u = edge_u; P.edge_v = edge_v; P.n_edges = n_edges;
+    P.degrees = degrees; P.regs = regs; P.n_rows = n_rows; P.slot = slot; P.has = has;
+    P.p = p; P.gamma = gamma;
+    P.pe_support = pe_support; P.pe_s_hat = pe_s_hat; P.pe_s_cl = pe_s_cl; P.pe_method = pe_method;
+    P.result = result;
+    return run_count(P, mode == 1 ? MODE_HYBRID : 2, details, ws, wsb, (cudaStream_t)stream);
+}
+
+TCHLL_EXPORT int tchll_hybrid_count_dense(const int32_t* row_ptr, int64_t n_nodes, const int32_t* col_idx,
+                                          int64_t nnz, const int32_t* edge_u, const int32_t* edge_v,
+                                          int64_t n_edges, const int32_t* degrees, const uint8_t* sketch_regs,
+                                          const uint8_t* has_sketch, int32_t p, int64_t gamma,
+                                          int32_t split_kernels, tchll_count_result* result, void* workspace,
+                                          size_t workspace_bytes, void* stream) {
+    return hybrid_common(row_ptr, n_nodes, col_idx, nnz, edge_u, edge_v, n_edges, degrees, sketch_regs,
+                         n_nodes, nullptr, has_sketch, p, gamma, split_kernels ? 2 : 1, nullptr, nullptr,
+                         nullptr, nullptr, result, workspace, workspace_bytes, stream);
+}
+
+TCHLL_EXPORT int tchll_hybrid_count_compact(const int32_t* row_ptr, int64_t n_nodes, const int32_t* col_idx,
+                                            int64_t nnz, const int32_t* edge_u, const int32_t* edge_v,
+                                            int64_t n_edges, const int32_t* degrees, const uint8_t* rows,
+                                            int64_t n_rows, const int64_t* slot, int32_t p, int64_t gamma,
+                                            int32_t split_kernels, int64_t* per_edge_support,
+                                            double* per_edge_s_hat, double* per_edge_s_clamped,
+                                            uint8_t* per_edge_method, tchll_count_result* result,
+                                            void* workspace, size_t workspace_bytes, void* stream) {
+    TCHLL_ARG(slot != nullptr || n_edges == 0, "slot is null");
+    return hybrid_common(row_ptr, n_nodes, col_idx, nnz, edge_u, edge_v, n_edges, degrees, rows, n_rows, slot,
+                         nullptr, p, gamma, split_kernels ? 2 : 1, per_edge_support, per_edge_s_hat,
+                         per_edge_s_clamped, per_edge_method, result, workspace, workspace_bytes, stream);
+}
+
+TCHLL_EXPORT int tchll_set_count_tuning(int32_t chunk, int32_t slots_log2, int32_t tiny, int32_t blocks_per_sm) {
+    TCHLL_ARG(chunk >= 32 && chunk % 32 == 0 && chunk <= (1 << 20), "chunk must be a multiple of 32 in [32, 2^20]");
+    TCHLL_ARG(slots_log2 >= 6 && slots_log2 <= 13, "slots_log2 must be in [6, 13]");
+    TCHLL_ARG(tiny >= 0 && tiny <= 4096, "tiny must be in [0, 4096]");
+    TCHLL_ARG(blocks_per_sm >= 0 && blocks_per_sm <= 32, "blocks_per_sm must be in [0, 32]");
+    g_tuning.chunk = chunk;
+    g_tuning.slots_log2 = slots_log2;
+    g_tuning.tiny = tiny;
+    g_tuning.blocks_per_sm = blocks_per_sm;
+    return TCHLL_OK;
+}
+
+TCHLL_EXPORT int tchll_get_count_tuning(int32_t* out4) {
+    TCHLL_ARG(out4 != nullptr, "out is null");
+    out4[0] = g_tuning.chunk;
+    out4[1] = g_tuning.slots_log2;
+    out4[2] = g_tuning.tiny;
+    out4[3] = g_tuning.blocks_per_sm;
+    return TCHLL_OK;
+}

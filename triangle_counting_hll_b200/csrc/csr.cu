@@ -1,0 +1,421 @@
+// csr.cu -- device construction of the oriented CSR.
+//
+// Reference semantics (ChitandaEruQ/triangle_counting_hll):
+//   load + dedup   src/graph.py:8-26 (canonical (min,max), self-loops dropped,
+//                  set semantics), experiment/exp_gpu.py:288-303 (np.unique)
+//   compaction     experiment/exp_gpu.py:317-323 (np.union1d of endpoints;
+//                  ids become ranks) == src/gpu_graph.py:19-37 node_index
+//   degree/orient  src/graph.py:41-54, experiment/exp_gpu.py:325-339:
+//                  u -> v iff (deg u, id u) < (deg v, id v); compaction is
+//                  monotone, so comparing compacted ids gives the same order
+//   CSR            experiment/exp_gpu.py:350-362 (np.lexsort by (src, dst))
+//
+// Pipeline: pack canonical pairs into 63-bit keys -> radix sort -> unique ->
+// endpoint ids sorted + unique (the node table) -> binary-search remap and
+// degree histogram -> orient -> radix sort by (src, dst) -> scan.  Sorting,
+// unique and scans use CUB (header templates compiled into this library); the
+// other passes are kernels written here.
+#include <cub/cub.cuh>
+
+#include "common.cuh"
+
+namespace tchll {
+
+// (2^31-1, 2^31-1) is never a canonical pair (min < max), so it marks dropped
+// self-loops and sorts after every real key.
+constexpr uint64_t kSentinel = (0x7FFFFFFFull << 32) | 0x7FFFFFFFull;
+constexpr uint32_t kEndSentinel = 0xFFFFFFFFu;
+
+struct CsrWs {
+    uint64_t* k0;
+    uint64_t* k1;
+    uint32_t* e0;
+    uint32_t* e1;
+    int32_t* deg;
+    int32_t* fdeg;
+    int32_t* ca;
+    int32_t* cb;
+    int64_t* cnt;  // [0] unique keys, [1] unique endpoints, [2] negative-id flag
+    void* tmp;
+    size_t tmp_bytes;
+};
+
+static size_t csr_cub_tmp(int64_t n_raw) {
+    const int R = (int)(n_raw > 0 ? n_raw : 1);
+    size_t a = 0, b = 0, c = 0, d = 0, e = 0;
+    cub::DeviceRadixSort::SortKeys(nullptr, a, (uint64_t*)nullptr, (uint64_t*)nullptr, R, 0, 63);
+    cub::DeviceSelect::Unique(nullptr, b, (uint64_t*)nullptr, (uint64_t*)nullptr, (int64_t*)nullptr, R);
+    cub::DeviceRadixSort::SortKeys(nullptr, c, (uint32_t*)nullptr, (uint32_t*)nullptr, 2 * R, 0, 32);
+    cub::DeviceSelect::Unique(nullptr, d, (uint32_t*)nullptr, (uint32_t*)nullptr, (int64_t*)nullptr, 2 * R);
+    cub::DeviceScan::ExclusiveSum(nullptr, e, (int32_t*)nullptr, (int32_t*)nullptr, 2 * R + 1);
+    size_t m = a;
+    if (b > m) m = b;
+    if (c > m) m = c;
+    if (d > m) m = d;
+    if (e > m) m = e;
+    return m;
+}
+
+static bool carve_csr(void* ws, size_t bytes, int64_t n_raw, CsrWs& W, size_t* need) {
+    const size_t R = (size_t)(n_raw > 0 ? n_raw : 1);
+    Carve cv(ws, bytes);
+    W.k0 = cv.take<uint64_t>(R);
+    W.k1 = cv.take<uint64_t>(R);
+    W.e0 = cv.take<uint32_t>(2 * R);
+    W.e1 = cv.take<uint32_t>(2 * R);
+    W.deg = cv.take<int32_t>(2 * R + 1);
+    W.fdeg = cv.take<int32_t>(2 * R + 2);
+    W.ca = cv.take<int32_t>(R);
+    W.cb = cv.take<int32_t>(R);
+    W.cnt = cv.take<int64_t>(4);
+    W.tmp_bytes = csr_cub_tmp(n_raw);
+    W.tmp = cv.take<char>(W.tmp_bytes);
+    if (need) *need = cv.off;
+    return cv.ok();
+}
+
+static int grid_n(int64_t n, int threads = 256) {
+    int64_t g = (n + threads - 1) / threads;
+    const int64_t cap = (int64_t)sm_count() * 32;
+    if (g > cap) g = cap;
+    return g < 1 ? 1 : (int)g;
+}
+
+#define GRID_STRIDE(i, n) \
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
+
+__global__ void canon_kernel(const int32_t* __restrict__ ru, const int32_t* __restrict__ rv, int64_t n,
+                             uint64_t* keys, int64_t* cnt) {
+    bool neg = false;
+    GRID_STRIDE(i, n) {
+        const int32_t u = ru[i], v = rv[i];
+        if (u < 0 || v < 0) {
+            neg = true;
+            keys[i] = kSentinel;
+            continue;
+        }
+        const uint32_t a = (uint32_t)(u < v ? u : v), b = (uint32_t)(u < v ? v : u);
+        keys[i] = (u == v) ? kSentinel : (((uint64_t)a << 32) | b);
+    }
+    if (neg) cnt[2] = 1;
+}
+
+// Endpoints of the unique keys (sentinels become kEndSentinel).
+__global__ void ends_kernel(const uint64_t* __restrict__ keys, int64_t cap, const int64_t* cnt, uint32_t* ends) {
+    const int64_t nk = cnt[0];
+    GRID_STRIDE(i, cap) {
+        uint64_t k = i < nk ? keys[i] : kSentinel;
+        if (k == kSentinel) {
+            ends[2 * i] = kEndSentinel;
+            ends[2 * i + 1] = kEndSentinel;
+        } else {
+            ends[2 * i] = (uint32_t)(k >> 32);
+            ends[2 * i + 1] = (uint32_t)(k & 0xFFFFFFFFu);
+        }
+    }
+}
+
+__device__ __forceinline__ int64_t lower_bound_u32(const uint32_t* a, int64_t n, uint32_t x) {
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (a[mid] < x) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+// Number of real edges / nodes: drop the trailing sentinel when present.
+__device__ __forceinline__ int64_t n_real_edges(const uint64_t* keys, const int64_t* cnt) {
+    const int64_t nk = cnt[0];
+    return (nk > 0 && keys[nk - 1] == kSentinel) ? nk - 1 : nk;
+}
+__device__ __forceinline__ int64_t n_real_nodes(const uint32_t* nodes, const int64_t* cnt) {
+    const int64_t nn = cnt[1];
+    return (nn > 0 && nodes[nn - 1] == kEndSentinel) ? nn - 1 : nn;
+}
+
+__global__ void remap_kernel(const uint64_t* __restrict__ keys, int64_t cap, const uint32_t* __restrict__ nodes,
+                             const int64_t* cnt, int32_t* ca, int32_t* cb, int32_t* deg) {
+    const int64_t ne = n_real_edges(keys, cnt);
+    const int64_t nn = n_real_nodes(nodes, cnt);
+    GRID_STRIDE(i, cap) {
+        if (i >= ne) break;
+        const uint64_t k = keys[i];
+        const int32_t a = (int32_t)lower_bound_u32(nodes, nn, (uint32_t)(k >> 32));
+        const int32_t b = (int32_t)lower_bound_u32(nodes, nn, (uint32_t)(k & 0xFFFFFFFFu));
+        ca[i] = a;
+        cb[i] = b;
+        atomicAdd(deg + a, 1);
+        atomicAdd(deg + b, 1);
+    }
+}
+
+__global__ void sizes_kernel(const uint64_t* keys, const uint32_t* nodes, const int64_t* cnt, int64_t* sizes) {
+    if (cnt[2]) {
+        sizes[0] = -1;
+        sizes[1] = -1;
+        return;
+    }
+    sizes[0] = n_real_nodes(nodes, cnt);
+    sizes[1] = n_real_edges(keys, cnt);
+}
+
+__global__ void orient_kernel(const int32_t* __restrict__ ca, const int32_t* __restrict__ cb, int64_t ne,
+                              const int32_t* __restrict__ deg, int32_t* fdeg, uint64_t* okeys) {
+    GRID_STRIDE(i, ne) {
+        const int32_t a = ca[i], b = cb[i];
+        const int32_t da = deg[a], db = deg[b];
+        const bool first = (da < db) || (da == db && a < b);
+        const int32_t s = first ? a : b, d = first ? b : a;
+        atomicAdd(fdeg + s, 1);
+        okeys[i] = ((uint64_t)(uint32_t)s << 32) | (uint32_t)d;
+    }
+}
+
+__global__ void split_kernel(const uint64_t* __restrict__ okeys, int64_t ne, int32_t* col_idx, int32_t* edge_u,
+                             int32_t* edge_v) {
+    GRID_STRIDE(i, ne) {
+        const uint64_t k = okeys[i];
+        const int32_t d = (int32_t)(k & 0xFFFFFFFFu);
+        edge_u[i] = (int32_t)(k >> 32);
+        col_idx[i] = d;
+        edge_v[i] = d;
+    }
+}
+
+__global__ void copy_nodes_kernel(const uint32_t* __restrict__ nodes, int64_t n, const int32_t* __restrict__ fdeg,
+                                  const int32_t* __restrict__ deg, int32_t* node_ids, int32_t* degrees,
+                                  int32_t* undirected) {
+    GRID_STRIDE(i, n) {
+        node_ids[i] = (int32_t)nodes[i];
+        degrees[i] = fdeg[i];
+        if (undirected) undirected[i] = deg[i];
+    }
+}
+
+static int bits_for(int64_t maxv) {
+    int b = 1;
+    while (b < 63 && (maxv >> b) != 0) ++b;
+    return b;
+}
+
+// ------------------------------------------------- forward_adj -> CSR ------
+__global__ void iota_kernel(int64_t* a, int64_t n) {
+    GRID_STRIDE(i, n) a[i] = i;
+}
+
+__global__ void gather_deg_kernel(const int64_t* __restrict__ lens, const int64_t* __restrict__ order, int64_t n,
+                                  int32_t* degrees, int32_t* deg_scan_in) {
+    GRID_STRIDE(i, n) {
+        const int32_t d = (int32_t)lens[order[i]];
+        degrees[i] = d;
+        deg_scan_in[i] = d;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) deg_scan_in[n] = 0;
+}
+
+__device__ __forceinline__ int64_t upper_bound_i32(const int32_t* a, int64_t n, int64_t x) {
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if ((int64_t)a[mid] <= x) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void adj_fill_kernel(const int64_t* __restrict__ sorted_keys, int64_t n,
+                                const int64_t* __restrict__ order, const int64_t* __restrict__ dict_off,
+                                const int32_t* __restrict__ row_ptr, const int64_t* __restrict__ values, int64_t nnz,
+                                int32_t* col_idx, int32_t* edge_u, int32_t* edge_v, unsigned long long* missing) {
+    unsigned long long miss = 0;
+    GRID_STRIDE(k, nnz) {
+        const int64_t row = upper_bound_i32(row_ptr, n + 1, k) - 1;
+        const int64_t src = dict_off[order[row]] + (k - row_ptr[row]);
+        const int64_t x = values[src];
+        int64_t lo = 0, hi = n;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi) >> 1;
+            if (sorted_keys[mid] < x) lo = mid + 1; else hi = mid;
+        }
+        int32_t c = (int32_t)lo;
+        if (lo >= n || sorted_keys[lo] != x) {
+            ++miss;
+            c = -1;
+        }
+        col_idx[k] = c;
+        edge_v[k] = c;
+        edge_u[k] = (int32_t)row;
+    }
+    if (miss) atomicAdd(missing, miss);
+}
+
+__global__ void zero_kernel(int64_t* p) { *p = 0; }
+
+}  // namespace tchll
+
+using namespace tchll;
+
+TCHLL_EXPORT int tchll_csr_workspace_bytes(int64_t n_raw, size_t* bytes) {
+    TCHLL_ARG(bytes && n_raw >= 0, "bad arguments");
+    TCHLL_ARG(n_raw < (int64_t)(INT32_MAX / 2), "edge list longer than 2^30 entries");
+    CsrWs W;
+    carve_csr(nullptr, 0, n_raw, W, bytes);
+    return TCHLL_OK;
+}
+
+TCHLL_EXPORT int tchll_csr_build_phase1(const int32_t* raw_u, const int32_t* raw_v, int64_t n_raw, int64_t* sizes,
+                                        void* workspace, size_t workspace_bytes, void* stream) {
+    TCHLL_ARG(sizes != nullptr && n_raw >= 0, "bad arguments");
+    TCHLL_ARG(n_raw == 0 || (raw_u && raw_v), "null edge arrays");
+    TCHLL_ARG(n_raw < (int64_t)(INT32_MAX / 2), "edge list longer than 2^30 entries");
+    CsrWs W;
+    size_t need = 0;
+    if (!carve_csr(workspace, workspace_bytes, n_raw, W, &need) || !workspace) {
+        set_error("workspace too small: need %zu bytes, have %zu", need, workspace_bytes);
+        return TCHLL_EWORKSPACE;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const int R = (int)(n_raw > 0 ? n_raw : 1);
+    TCHLL_CUDA(cudaMemsetAsync(W.cnt, 0, 4 * sizeof(int64_t), st));
+    TCHLL_CUDA(cudaMemsetAsync(W.deg, 0, (2 * (size_t)R + 1) * sizeof(int32_t), st));
+    if (n_raw == 0) {
+        TCHLL_CUDA(cudaMemsetAsync(sizes, 0, 2 * sizeof(int64_t), st));
+        return TCHLL_OK;
+    }
+    canon_kernel<<<grid_n(n_raw), 256, 0, st>>>(raw_u, raw_v, n_raw, W.k0, W.cnt);
+    TCHLL_CHECK_LAUNCH("canon_kernel");
+    size_t tb = W.tmp_bytes;
+    TCHLL_CUDA(cub::DeviceRadixSort::SortKeys(W.tmp, tb, W.k0, W.k1, R, 0, 63, st));
+    count_launch();
+    tb = W.tmp_bytes;
+    TCHLL_CUDA(cub::DeviceSelect::Unique(W.tmp, tb, W.k1, W.k0, W.cnt + 0, R, st));
+    count_launch();
+    ends_kernel<<<grid_n(n_raw), 256, 0, st>>>(W.k0, n_raw, W.cnt, W.e0);
+    TCHLL_CHECK_LAUNCH("ends_kernel");
+    tb = W.tmp_bytes;
+    TCHLL_CUDA(cub::DeviceRadixSort::SortKeys(W.tmp, tb, W.e0, W.e1, 2 * R, 0, 32, st));
+    count_launch();
+    tb = W.tmp_bytes;
+    TCHLL_CUDA(cub::DeviceSelect::Unique(W.tmp, tb, W.e1, W.e0, W.cnt + 1, 2 * R, st));
+    count_launch();
+    remap_kernel<<<grid_n(n_raw), 256, 0, st>>>(W.k0, n_raw, W.e0, W.cnt, W.ca, W.cb, W.deg);
+    TCHLL_CHECK_LAUNCH("remap_kernel");
+    sizes_kernel<<<1, 1, 0, st>>>(W.k0, W.e0, W.cnt, sizes);
+    TCHLL_CHECK_LAUNCH("sizes_kernel");
+    return TCHLL_OK;
+}
+
+TCHLL_EXPORT int tchll_csr_build_phase2(int64_t n_raw, int64_t n_nodes, int64_t n_edges, int32_t* row_ptr,
+                                        int32_t* col_idx, int32_t* degrees, int32_t* node_ids, int32_t* edge_u,
+                                        int32_t* edge_v, int32_t* undirected_degrees, void* workspace,
+                                        size_t workspace_bytes, void* stream) {
+    TCHLL_ARG(n_nodes >= 0 && n_edges >= 0 && n_edges <= n_raw && n_nodes <= 2 * n_raw, "sizes out of range");
+    TCHLL_ARG(row_ptr != nullptr, "row_ptr is null");
+    TCHLL_ARG(n_nodes == 0 || (degrees && node_ids), "null node outputs");
+    TCHLL_ARG(n_edges == 0 || (col_idx && edge_u && edge_v), "null edge outputs");
+    CsrWs W;
+    size_t need = 0;
+    if (!carve_csr(workspace, workspace_bytes, n_raw, W, &need) || !workspace) {
+        set_error("workspace too small: need %zu bytes, have %zu", need, workspace_bytes);
+        return TCHLL_EWORKSPACE;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    TCHLL_CUDA(cudaMemsetAsync(W.fdeg, 0, ((size_t)n_nodes + 1) * sizeof(int32_t), st));
+    if (n_edges > 0) {
+        orient_kernel<<<grid_n(n_edges), 256, 0, st>>>(W.ca, W.cb, n_edges, W.deg, W.fdeg, W.k1);
+        TCHLL_CHECK_LAUNCH("orient_kernel");
+        size_t tb = W.tmp_bytes;
+        const int end_bit = 32 + bits_for(n_nodes > 1 ? n_nodes - 1 : 1);
+        TCHLL_CUDA(cub::DeviceRadixSort::SortKeys(W.tmp, tb, W.k1, W.k0, (int)n_edges, 0, end_bit, st));
+        count_launch();
+        split_kernel<<<grid_n(n_edges), 256, 0, st>>>(W.k0, n_edges, col_idx, edge_u, edge_v);
+        TCHLL_CHECK_LAUNCH("split_kernel");
+    }
+    size_t tb = W.tmp_bytes;
+    TCHLL_CUDA(cub::DeviceScan::ExclusiveSum(W.tmp, tb, W.fdeg, row_ptr, (int)(n_nodes + 1), st));
+    count_launch();
+    if (n_nodes > 0) {
+        copy_nodes_kernel<<<grid_n(n_nodes), 256, 0, st>>>(W.e0, n_nodes, W.fdeg, W.deg, node_ids, degrees,
+                                                            undirected_degrees);
+        TCHLL_CHECK_LAUNCH("copy_nodes_kernel");
+    }
+    return TCHLL_OK;
+}
+
+TCHLL_EXPORT int tchll_adj_workspace_bytes(int64_t n, int64_t nnz, size_t* bytes) {
+    TCHLL_ARG(bytes && n >= 0 && nnz >= 0, "bad arguments");
+    TCHLL_ARG(n < (int64_t)INT32_MAX - 1 && nnz <= (int64_t)INT32_MAX, "int32 CSR limits exceeded");
+    const int N = (int)(n > 0 ? n : 1);
+    size_t a = 0, b = 0, c = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, a, (int64_t*)nullptr, (int64_t*)nullptr, N + 1);
+    cub::DeviceRadixSort::SortPairs(nullptr, b, (int64_t*)nullptr, (int64_t*)nullptr, (int64_t*)nullptr,
+                                    (int64_t*)nullptr, N);
+    cub::DeviceScan::ExclusiveSum(nullptr, c, (int32_t*)nullptr, (int32_t*)nullptr, N + 1);
+    size_t m = a > b ? a : b;
+    if (c > m) m = c;
+    Carve cv(nullptr, 0);
+    cv.take<int64_t>((size_t)N + 1);  // dict offsets
+    cv.take<int64_t>((size_t)N + 1);  // lens copy with trailing 0
+    cv.take<int64_t>((size_t)N);      // iota
+    cv.take<int32_t>((size_t)N + 1);  // degree scan input
+    cv.take<char>(m);
+    *bytes = cv.off;
+    return TCHLL_OK;
+}
+
+TCHLL_EXPORT int tchll_csr_from_adjacency(const int64_t* keys, const int64_t* lens, int64_t n,
+                                          const int64_t* values, int64_t nnz, int64_t* node_ids, int32_t* row_ptr,
+                                          int32_t* degrees, int32_t* col_idx, int32_t* edge_u, int32_t* edge_v,
+                                          int64_t* order, int64_t* missing, void* workspace, size_t workspace_bytes,
+                                          void* stream) {
+    TCHLL_ARG(n >= 0 && nnz >= 0, "negative size");
+    TCHLL_ARG(row_ptr && missing, "null output");
+    TCHLL_ARG(n == 0 || (keys && lens && node_ids && degrees && order), "null node arrays");
+    TCHLL_ARG(nnz == 0 || (values && col_idx && edge_u && edge_v), "null edge arrays");
+    size_t need = 0;
+    int rc = tchll_adj_workspace_bytes(n, nnz, &need);
+    if (rc) return rc;
+    TCHLL_ARG(workspace != nullptr && workspace_bytes >= need, "workspace too small: need %zu bytes", need);
+    const int N = (int)(n > 0 ? n : 1);
+    size_t a = 0, b = 0, c = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, a, (int64_t*)nullptr, (int64_t*)nullptr, N + 1);
+    cub::DeviceRadixSort::SortPairs(nullptr, b, (int64_t*)nullptr, (int64_t*)nullptr, (int64_t*)nullptr,
+                                    (int64_t*)nullptr, N);
+    cub::DeviceScan::ExclusiveSum(nullptr, c, (int32_t*)nullptr, (int32_t*)nullptr, N + 1);
+    size_t m = a > b ? a : b;
+    if (c > m) m = c;
+    Carve cv(workspace, workspace_bytes);
+    int64_t* dict_off = cv.take<int64_t>((size_t)N + 1);
+    int64_t* lens0 = cv.take<int64_t>((size_t)N + 1);
+    int64_t* iota = cv.take<int64_t>((size_t)N);
+    int32_t* dscan = cv.take<int32_t>((size_t)N + 1);
+    void* tmp = cv.take<char>(m);
+    cudaStream_t st = (cudaStream_t)stream;
+    zero_kernel<<<1, 1, 0, st>>>(missing);
+    TCHLL_CHECK_LAUNCH("zero_kernel");
+    if (n == 0) {
+        TCHLL_CUDA(cudaMemsetAsync(row_ptr, 0, sizeof(int32_t), st));
+        return TCHLL_OK;
+    }
+    TCHLL_CUDA(cudaMemcpyAsync(lens0, lens, sizeof(int64_t) * n, cudaMemcpyDeviceToDevice, st));
+    TCHLL_CUDA(cudaMemsetAsync(lens0 + n, 0, sizeof(int64_t), st));
+    size_t tb = m;
+    TCHLL_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, lens0, dict_off, (int)(n + 1), st));
+    count_launch();
+    iota_kernel<<<grid_n(n), 256, 0, st>>>(iota, n);
+    TCHLL_CHECK_LAUNCH("iota_kernel");
+    tb = m;
+    TCHLL_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, keys, node_ids, iota, order, (int)n, 0, 64, st));
+    count_launch();
+    gather_deg_kernel<<<grid_n(n), 256, 0, st>>>(lens, order, n, degrees, dscan);
+    TCHLL_CHECK_LAUNCH("gather_deg_kernel");
+    tb = m;
+    TCHLL_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, dscan, row_ptr, (int)(n + 1), st));
+    count_launch();
+    if (nnz > 0) {
+        adj_fill_kernel<<<grid_n(nnz), 256, 0, st>>>(node_ids, n, order, dict_off, row_ptr, values, nnz, col_idx,
+                                                    edge_u, edge_v, (unsigned long long*)missing);
+        TCHLL_CHECK_LAUNCH("adj_fill_kernel");
+    }
+    return TCHLL_OK;
+}
