@@ -70,8 +70,9 @@ int tchll_version(void);
 uint64_t tchll_launch_count(void);
 
 /* --------------------------------------------- exact / hybrid counting --- */
-/* Workspace for tchll_exact_count / tchll_hybrid_count_*. */
-int tchll_count_workspace_bytes(int64_t n_edges, size_t* bytes);
+/* Workspace for tchll_exact_count / tchll_hybrid_count_* on a CSR of n_nodes
+ * rows and n_edges edges (holds the reoriented pair list: 8 bytes per edge). */
+int tchll_count_workspace_bytes(int64_t n_nodes, int64_t n_edges, size_t* bytes);
 
 /*
  * Exact count: T = sum over the n_edges edges (edge_u[i], edge_v[i]) of
@@ -116,13 +117,18 @@ int tchll_hybrid_count_compact(const int32_t* row_ptr, int64_t n_nodes, const in
                                tchll_count_result* result, void* workspace, size_t workspace_bytes,
                                void* stream);
 
-/* Launch shape of the counting kernels (host state; no counterpart in the
- * reference, whose block size is fixed at 256, src/gpu_hybrid.py:13).
- * chunk: edges claimed per warp (multiple of 32); slots_log2: per-warp hash
- * table capacity; tiny: lane-local merge threshold on |N+u|+|N+v|;
- * blocks_per_sm: 0 = occupancy maximum.  out4 receives the same four. */
+/* Launch shape of the counting kernels (process-wide host state; no
+ * counterpart in the reference, whose block size is fixed at 256,
+ * src/gpu_hybrid.py:13).  chunk: edges claimed per warp (multiple of 32);
+ * slots_log2: per-warp hash table capacity; tiny: lane-local merge threshold
+ * on |N+u|+|N+v|; blocks_per_sm: 0 = occupancy maximum; warps_per_cta: 1-8;
+ * pairs: 1 = probe the shorter list into a table of the longer one (edges
+ * regrouped by a device counting sort), 0 = edges as given.  out6 receives
+ * chunk, slots_log2, tiny, blocks_per_sm, warps_per_cta, pairs.  Results are
+ * identical for every setting. */
 int tchll_set_count_tuning(int32_t chunk, int32_t slots_log2, int32_t tiny, int32_t blocks_per_sm);
-int tchll_get_count_tuning(int32_t* out4 /* host */);
+int tchll_set_count_shape(int32_t warps_per_cta, int32_t pairs);
+int tchll_get_count_tuning(int32_t* out6 /* host */);
 
 /* ------------------------------------------------------------ sketches --- */
 /*

@@ -178,7 +178,7 @@ def test_tuning_does_not_change_results(tchll, oracle, dev):
     base = core.get_count_tuning()
     outs = []
     try:
-        for chunk, lg, tiny in ((64, 11, 16), (32, 8, 0), (256, 12, 64), (1024, 13, 4)):
+        for chunk, lg, tiny in ((64, 11, 16), (32, 8, 0), (256, 12, 64), (1024, 12, 4)):
             core.set_count_tuning(chunk, lg, tiny, 0)
             res, _ = core.hybrid_count_compact_tensors(g.row_ptr, g.col_idx, g.edge_u, g.edge_v, g.degrees, rows,
                                                        slot, 10, 32)

@@ -58,13 +58,14 @@ SIGNATURES = {
     "tchll_last_error": (C.c_char_p, []),
     "tchll_version": (C.c_int, []),
     "tchll_launch_count": (_U64, []),
-    "tchll_count_workspace_bytes": (C.c_int, [_I64, C.POINTER(_SZ)]),
+    "tchll_count_workspace_bytes": (C.c_int, [_I64, _I64, C.POINTER(_SZ)]),
     "tchll_exact_count": (C.c_int, [_P, _I64, _P, _I64, _P, _P, _I64, _P, _P, _P, _SZ, _P]),
     "tchll_hybrid_count_dense": (C.c_int, [_P, _I64, _P, _I64, _P, _P, _I64, _P, _P, _P, _I32, _I64, _I32,
                                            _P, _P, _SZ, _P]),
     "tchll_hybrid_count_compact": (C.c_int, [_P, _I64, _P, _I64, _P, _P, _I64, _P, _P, _I64, _P, _I32, _I64,
                                              _I32, _P, _P, _P, _P, _P, _P, _SZ, _P]),
     "tchll_set_count_tuning": (C.c_int, [_I32, _I32, _I32, _I32]),
+    "tchll_set_count_shape": (C.c_int, [_I32, _I32]),
     "tchll_get_count_tuning": (C.c_int, [_P]),
     "tchll_sketch_workspace_bytes": (C.c_int, [_I64, C.POINTER(_SZ)]),
     "tchll_build_sketches_dense": (C.c_int, [_P, _I64, _P, _I64, _I64, _I32, _P, _P, _P]),

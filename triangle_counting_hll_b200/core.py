@@ -169,9 +169,9 @@ def adjacency_with_missing_nodes(forward_adj: dict, device=None) -> AdjacencyCSR
 
 
 # ------------------------------------------------------------- counting (a3)
-def _count_ws(n_edges: int, device) -> torch.Tensor:
+def _count_ws(n_nodes: int, n_edges: int, device) -> torch.Tensor:
     nb = C.c_size_t(0)
-    check(load().tchll_count_workspace_bytes(int(n_edges), C.byref(nb)))
+    check(load().tchll_count_workspace_bytes(int(n_nodes), int(n_edges), C.byref(nb)))
     return _ws(nb.value, device)
 
 
@@ -187,7 +187,7 @@ def exact_count_tensors(row_ptr: torch.Tensor, col_idx: torch.Tensor, edge_u: to
         raise ValueError("edge_u and edge_v differ in length")
     res = result if result is not None else _lib.count_result_tensor(dev)
     pe = torch.empty(n_edges, dtype=torch.int64, device=dev) if per_edge else None
-    ws = _count_ws(n_edges, dev)
+    ws = _count_ws(n_nodes, n_edges, dev)
     check(load().tchll_exact_count(ptr(row_ptr), n_nodes, ptr(col_idx), int(col_idx.numel()), ptr(edge_u),
                                    ptr(edge_v), n_edges, ptr(pe), ptr(res), ptr(ws), ws.numel(),
                                    stream_handle(dev)), "exact count")
@@ -206,7 +206,7 @@ def hybrid_count_dense_tensors(row_ptr, col_idx, edge_u, edge_v, degrees, sketch
     if int(has_sketch.numel()) < n_nodes or int(degrees.numel()) < n_nodes:
         raise ValueError("has_sketch / degrees shorter than n_nodes")
     res = result if result is not None else _lib.count_result_tensor(dev)
-    ws = _count_ws(n_edges, dev)
+    ws = _count_ws(n_nodes, n_edges, dev)
     check(load().tchll_hybrid_count_dense(ptr(row_ptr), n_nodes, ptr(col_idx), int(col_idx.numel()),
                                           ptr(edge_u), ptr(edge_v), n_edges, ptr(degrees), ptr(sketch_regs),
                                           ptr(has_sketch), int(p), int(gamma), 1 if split_kernels else 0,
@@ -230,7 +230,7 @@ def hybrid_count_compact_tensors(row_ptr, col_idx, edge_u, edge_v, degrees, rows
               torch.empty(n_edges, dtype=torch.float64, device=dev),
               torch.empty(n_edges, dtype=torch.float64, device=dev),
               torch.empty(n_edges, dtype=torch.uint8, device=dev))
-    ws = _count_ws(n_edges, dev)
+    ws = _count_ws(n_nodes, n_edges, dev)
     pp = [ptr(t) for t in pe] if pe else [None, None, None, None]
     check(load().tchll_hybrid_count_compact(ptr(row_ptr), n_nodes, ptr(col_idx), int(col_idx.numel()),
                                             ptr(edge_u), ptr(edge_v), n_edges, ptr(degrees), ptr(rows), n_rows,
@@ -240,14 +240,24 @@ def hybrid_count_compact_tensors(row_ptr, col_idx, edge_u, edge_v, degrees, rows
     return res, pe
 
 
-def set_count_tuning(chunk: int = 64, slots_log2: int = 11, tiny: int = 16, blocks_per_sm: int = 0) -> None:
-    check(load().tchll_set_count_tuning(int(chunk), int(slots_log2), int(tiny), int(blocks_per_sm)))
+def set_count_tuning(chunk: int = 64, slots_log2: int = 11, tiny: int = 16, blocks_per_sm: int = 0,
+                     warps: Optional[int] = None, pairs: Optional[bool] = None) -> None:
+    """Launch shape of the counting kernels (results do not depend on it)."""
+    L = load()
+    cur = get_count_tuning()
+    w = cur["warps"] if warps is None else int(warps)
+    pr = cur["pairs"] if pairs is None else int(bool(pairs))
+    # one warp fits every table size, so go through it to reach any valid shape
+    check(L.tchll_set_count_shape(1, pr))
+    check(L.tchll_set_count_tuning(int(chunk), int(slots_log2), int(tiny), int(blocks_per_sm)))
+    check(L.tchll_set_count_shape(w, pr))
 
 
 def get_count_tuning() -> dict:
-    out = (C.c_int32 * 4)()
+    out = (C.c_int32 * 6)()
     check(load().tchll_get_count_tuning(C.cast(out, C.c_void_p)))
-    return {"chunk": out[0], "slots_log2": out[1], "tiny": out[2], "blocks_per_sm": out[3]}
+    return {"chunk": out[0], "slots_log2": out[1], "tiny": out[2], "blocks_per_sm": out[3], "warps": out[4],
+            "pairs": out[5]}
 
 
 # ----------------------------------------------------------- sketches (a4)

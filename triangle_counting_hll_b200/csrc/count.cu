@@ -10,26 +10,34 @@
 //            estimated from the register-wise max of the two sketches with the
 //            reference's bias and range corrections (src/hll.py:37-54,112-120).
 //
-// Design (one persistent launch, work stealing over edge chunks):
-//   * A warp claims CHUNK consecutive edges with one atomicAdd and walks them
-//     32 at a time.  Within a batch, edges that share u form a group; the warp
-//     keeps N+(u) in a private shared-memory hash table (open addressing,
-//     load <= 1/4 where the capacity allows) that survives across groups and
-//     batches while u does not change, so a CSR-ordered edge list builds each
-//     row's table about once per chunk.
-//   * The group's probe lists N+(v) are flattened into one stream of 16-byte
-//     quads and dealt to the 32 lanes with a warp scan, so short and long
-//     lists keep every lane busy.  Each element costs one hash probe.
-//   * Edges whose two lists are both tiny are merged lane-locally; rows too
-//     long for a warp table fall back to a warp binary search.
-//   * HLL edges: the warp reads both 2^p-byte register rows with 16-byte loads,
-//     merges them with __vmaxu4 and accumulates sum 2^-r EXACTLY as a 128-bit
-//     fixed-point integer (zero registers counted with __vcmpeq4), then one
-//     lane applies alpha*m^2/Z, linear counting and the 2^64 correction in
-//     FP64, clamps, and adds the result in 2^-32 fixed point.
-//   * All totals are integers (uint64 exact count, 128-bit fixed-point HLL sum,
-//     int64 stats) added with integer atomics, so results do not depend on
-//     scheduling: any partition of the edges gives bit-identical totals.
+// Design
+//   * Table side / probe side.  |N+(u) cap N+(v)| is symmetric, so each exact
+//     edge becomes a pair (x, y) with x the endpoint of the LONGER list: a
+//     device counting sort (histogram, scan, scatter) groups the pairs by x.
+//     A warp then keeps N+(x) in a private shared-memory hash table while it
+//     streams the shorter N+(y) lists through it: the probe count drops from
+//     sum d+(v) to sum min(d+u, d+v) (43.4 G list elements -> 11.8 G probes on
+//     R-MAT scale 22).  Per-edge outputs (details) use the edges as given.
+//   * One persistent launch, work stealing: a warp claims CHUNK consecutive
+//     pairs with one atomicAdd and walks them 32 at a time; pairs sharing x
+//     form a group and reuse the warp's table (built once per group per chunk).
+//   * The table is bucketized cuckoo hashing (two hash functions, two-slot
+//     buckets, load <= 1/2): a lookup is two 8-byte shared loads and four
+//     compares, with no probe chains to diverge on.
+//   * The group's probe lists are flattened into one stream of 16-byte quads
+//     dealt to the 32 lanes by a warp scan, so short and long lists keep
+//     every lane busy.
+//   * Tiny pairs are merged lane-locally; tables too large for a warp fall
+//     back to a warp binary search.
+//   * HLL edges: the warp reads both 2^p-byte register rows with 16-byte
+//     loads, merges them with __vmaxu4 and accumulates sum 2^-r EXACTLY as a
+//     128-bit fixed-point integer; one lane applies the FP64 corrections,
+//     clamps and adds the result in 2^-32 fixed point.
+//   * Every total is an integer (uint64 exact count, 128-bit fixed-point HLL
+//     sum, int64 stats) added with integer atomics, so results do not depend
+//     on scheduling or partitioning: they are bit-identical run to run.
+#include <cub/cub.cuh>
+
 #include "common.cuh"
 #include "hll_device.cuh"
 
@@ -38,9 +46,9 @@ namespace tchll {
 enum : int { MODE_EXACT = 0, MODE_HYBRID = 1, MODE_HYB_EXACT = 2, MODE_HYB_HLL = 3 };
 
 enum : uint32_t {
-    ST_BAD_EDGE = 1u,   // edge endpoint outside [0, n_nodes)
-    ST_BAD_ROW = 2u,    // row_ptr extent outside [0, nnz] or decreasing
-    ST_BAD_SLOT = 4u,   // sketch slot outside [0, n_rows)
+    ST_BAD_EDGE = 1u,  // edge endpoint outside [0, n_nodes)
+    ST_BAD_ROW = 2u,   // row_ptr extent outside [0, nnz] or decreasing
+    ST_BAD_SLOT = 4u,  // sketch slot outside [0, n_rows)
 };
 
 struct CountParams {
@@ -51,53 +59,179 @@ struct CountParams {
     const int32_t* edge_u;
     const int32_t* edge_v;
     int64_t n_edges;
-    const int32_t* degrees;  // forward degree for routing (hybrid modes)
-    const uint8_t* regs;     // register rows
-    int64_t n_rows;          // rows available in regs
-    const int64_t* slot;     // compact layout: row of v, or -1; null -> dense
-    const uint8_t* has;      // dense layout: has_sketch[v] == 1 -> row v
+    const int32_t* n_edges_dev;  // when set, the edge count is read here (pairs)
+    const int32_t* degrees;      // forward degree for routing (hybrid modes)
+    const uint8_t* regs;         // register rows
+    int64_t n_rows;              // rows available in regs
+    const int64_t* slot;         // compact layout: row of v, or -1; null -> dense
+    const uint8_t* has;          // dense layout: has_sketch[v] == 1 -> row v
     int p;
     int64_t gamma;
-    int64_t* pe_support;     // per-edge exact support (details), zeroed by host
-    double* pe_s_hat;        // per-edge HLL s_hat (details)
-    double* pe_s_cl;         // per-edge HLL clamped support (details)
-    uint8_t* pe_method;      // per-edge 0 exact / 1 hll (details)
+    int64_t* pe_support;  // per-edge exact support (details), zeroed by host
+    double* pe_s_hat;     // per-edge HLL s_hat (details)
+    double* pe_s_cl;      // per-edge HLL clamped support (details)
+    uint8_t* pe_method;   // per-edge 0 exact / 1 hll (details)
     tchll_count_result* result;
     unsigned long long* work;
     int chunk;
-    int slots_log2;          // per-warp table capacity (log2 slots)
-    int tiny;                // lane-local merge when |N+u| + |N+v| <= tiny
+    int slots_log2;  // per-warp table capacity (log2 slots)
+    int tiny;        // lane-local merge when |N+x| + |N+y| <= tiny
 };
 
-__device__ __forceinline__ uint32_t tbl_hash(int32_t x, int lg) {
-    return ((uint32_t)x * 0x9E3779B1u) >> (32 - lg);
+// Bucketized cuckoo table: 2^lgb buckets of two int32 slots (one 8-byte
+// shared-memory word each); key x lives in bucket b1(x) or b2(x).  A lookup
+// is exactly two 8-byte loads and four compares -- no probe chains, so no
+// lane waits on another's collisions.
+struct Buckets {
+    uint32_t b1, b2;
+};
+
+__device__ __forceinline__ Buckets tbl_buckets(int32_t x, int lgb) {
+    const uint64_t h = (uint64_t)(uint32_t)x * 0x9E3779B97F4A7C15ull;
+    Buckets r;
+    r.b1 = (uint32_t)(h >> (64 - lgb));
+    r.b2 = (uint32_t)(h >> (32 - lgb)) & ((1u << lgb) - 1u);
+    if (r.b2 == r.b1) r.b2 ^= 1u;
+    return r;
 }
 
-__device__ __forceinline__ int tbl_probe(const int32_t* table, int lg, int32_t x) {
-    const uint32_t mask = (1u << lg) - 1u;
-    uint32_t h = tbl_hash(x, lg);
-    while (true) {
-        int32_t y = table[h];
-        if (y == x) return 1;
-        if (y < 0) return 0;
-        h = (h + 1u) & mask;
+__device__ __forceinline__ uint32_t tbl_lookup(const int2* T, int32_t x, int lgb) {
+    const Buckets b = tbl_buckets(x, lgb);
+    const int2 p = T[b.b1];
+    const int2 q = T[b.b2];
+    return (uint32_t)((p.x == x) | (p.y == x) | (q.x == x) | (q.y == x));
+}
+
+// Inserts x (lane-parallel, shared-memory atomics).  Returns false when the
+// key could not be placed within the kick budget (the caller then falls back
+// to binary search for this table side).
+__device__ __forceinline__ bool tbl_insert(int32_t* T, int32_t x, int lgb) {
+    int32_t cur = x;
+    uint32_t b = tbl_buckets(cur, lgb).b1;
+    for (int kick = 0; kick < 96; ++kick) {
+        if (atomicCAS(T + 2 * b, -1, cur) == -1) return true;
+        if (atomicCAS(T + 2 * b + 1, -1, cur) == -1) return true;
+        const Buckets cb = tbl_buckets(cur, lgb);
+        const uint32_t alt = (b == cb.b1) ? cb.b2 : cb.b1;
+        if (atomicCAS(T + 2 * alt, -1, cur) == -1) return true;
+        if (atomicCAS(T + 2 * alt + 1, -1, cur) == -1) return true;
+        // both buckets full: evict a resident of alt and move it to its
+        // other bucket (slots never return to empty, so victim >= 0)
+        const int32_t victim = atomicExch(T + 2 * alt + (kick & 1), cur);
+        cur = victim;
+        const Buckets vb = tbl_buckets(cur, lgb);
+        b = (alt == vb.b1) ? vb.b2 : vb.b1;
     }
+    return false;
 }
 
 __device__ __forceinline__ int ceil_log2_i(int x) { return x <= 1 ? 0 : 32 - __clz(x - 1); }
 
+// Loads and validates edge e; returns false (and flags status) when malformed.
+__device__ __forceinline__ bool load_edge(const CountParams& P, int64_t e, int32_t& u, int32_t& v, int32_t& us,
+                                          int32_t& ue, int32_t& vs, int32_t& ve, uint32_t& status) {
+    u = __ldg(P.edge_u + e);
+    v = __ldg(P.edge_v + e);
+    if (u < 0 || v < 0 || (int64_t)u >= P.n_nodes || (int64_t)v >= P.n_nodes) {
+        status |= ST_BAD_EDGE;
+        return false;
+    }
+    us = __ldg(P.row_ptr + u);
+    ue = __ldg(P.row_ptr + u + 1);
+    vs = __ldg(P.row_ptr + v);
+    ve = __ldg(P.row_ptr + v + 1);
+    if (us < 0 || ue < us || (int64_t)ue > P.nnz || vs < 0 || ve < vs || (int64_t)ve > P.nnz) {
+        status |= ST_BAD_ROW;
+        return false;
+    }
+    return true;
+}
+
+// Hybrid routing (src/hybrid.py:107-115): wants = min(deg) >= gamma,
+// both = both endpoints have a sketch.  Returns false on a bad slot.
+__device__ __forceinline__ bool route(const CountParams& P, int32_t u, int32_t v, int32_t& du, int32_t& dv,
+                                      int64_t& su, int64_t& sv, bool& wants, bool& both, uint32_t& status) {
+    du = __ldg(P.degrees + u);
+    dv = __ldg(P.degrees + v);
+    const int64_t proxy = du < dv ? du : dv;
+    wants = proxy >= P.gamma;
+    if (P.slot) {
+        su = __ldg(P.slot + u);
+        sv = __ldg(P.slot + v);
+    } else {
+        su = __ldg(P.has + u) == 1 ? (int64_t)u : -1;
+        sv = __ldg(P.has + v) == 1 ? (int64_t)v : -1;
+    }
+    if (su >= P.n_rows || sv >= P.n_rows) {
+        status |= ST_BAD_SLOT;
+        return false;
+    }
+    both = su >= 0 && sv >= 0;
+    return true;
+}
+
+// ------------------------------------------------------------ pair build ----
+// Exact edges (all edges, or in hybrid mode the exact-routed ones) become
+// pairs (x, y), x the endpoint with the longer forward list (ties: u).
+template <bool HYB>
+__device__ __forceinline__ bool pair_of(const CountParams& P, int64_t e, int32_t& x, int32_t& y, uint32_t& status) {
+    int32_t u, v, us, ue, vs, ve;
+    if (!load_edge(P, e, u, v, us, ue, vs, ve, status)) return false;
+    if (HYB) {
+        int32_t du, dv;
+        int64_t su, sv;
+        bool wants, both;
+        if (!route(P, u, v, du, dv, su, sv, wants, both, status)) return false;
+        if (wants && both) return false;  // HLL-routed
+    }
+    const bool ux = (ue - us) >= (ve - vs);
+    x = ux ? u : v;
+    y = ux ? v : u;
+    return true;
+}
+
+template <bool HYB>
+__global__ void pair_hist_kernel(const CountParams P, int32_t* cnt) {
+    uint32_t status = 0;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < P.n_edges;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        int32_t x, y;
+        if (pair_of<HYB>(P, e, x, y, status)) atomicAdd(cnt + x, 1);
+    }
+    if (status) atomicOr(&P.result->status, status);
+}
+
+template <bool HYB>
+__global__ void pair_scatter_kernel(const CountParams P, int32_t* cursor, int32_t* px, int32_t* py) {
+    uint32_t status = 0;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < P.n_edges;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        int32_t x, y;
+        if (pair_of<HYB>(P, e, x, y, status)) {
+            const int32_t pos = atomicAdd(cursor + x, 1);
+            px[pos] = x;
+            py[pos] = y;
+        }
+    }
+}
+
 // Warp-cooperative binary-search intersection count of two sorted lists in
-// global memory (used for rows too long for a warp table).  Returns per-lane
-// partial counts.
-__device__ __forceinline__ uint32_t warp_bsearch_count(const int32_t* a, int la, const int32_t* b, int lb,
-                                                       int lane) {
-    if (la > lb) { const int32_t* t = a; a = b; b = t; int tl = la; la = lb; lb = tl; }
+// global memory (tables too large for a warp).  Per-lane partial counts.
+__device__ __forceinline__ uint32_t warp_bsearch_count(const int32_t* a, int la, const int32_t* b, int lb, int lane) {
+    if (la > lb) {
+        const int32_t* t = a;
+        a = b;
+        b = t;
+        const int tl = la;
+        la = lb;
+        lb = tl;
+    }
     uint32_t c = 0;
     for (int i = lane; i < la; i += 32) {
-        int32_t x = __ldg(a + i);
+        const int32_t x = __ldg(a + i);
         int lo = 0, hi = lb;
         while (lo < hi) {
-            int mid = (lo + hi) >> 1;
+            const int mid = (lo + hi) >> 1;
             if (__ldg(b + mid) < x) lo = mid + 1; else hi = mid;
         }
         c += (lo < lb && __ldg(b + lo) == x);
@@ -109,7 +243,7 @@ __device__ __forceinline__ uint32_t lane_merge_count(const int32_t* a, int la, c
     int i = 0, j = 0;
     uint32_t c = 0;
     while (i < la && j < lb) {
-        int32_t x = __ldg(a + i), y = __ldg(b + j);
+        const int32_t x = __ldg(a + i), y = __ldg(b + j);
         c += (x == y);
         i += (x <= y);
         j += (y <= x);
@@ -123,66 +257,40 @@ __global__ void __launch_bounds__(256, 1) count_kernel(const CountParams P) {
     const int lane = threadIdx.x & 31;
     const int wid = threadIdx.x >> 5;
     const int cap_lg = P.slots_log2;
-    const int cap_keys = 1 << (cap_lg - 1);
+    const int cap_keys = 1 << (cap_lg - 1);  // load <= 1/2 in 2^cap_lg slots
     int32_t* table = smem + ((size_t)wid << cap_lg);
 
-    const int32_t* __restrict__ row_ptr = P.row_ptr;
     const int32_t* __restrict__ col_idx = P.col_idx;
+    const int64_t n_edges = P.n_edges_dev ? (int64_t)*P.n_edges_dev : P.n_edges;
 
     uint64_t acc = 0;
     U128 hacc;
     int64_t n_approx = 0, n_exact = 0, n_fallback = 0, n_clamped = 0;
     uint32_t status = 0;
     int cur_u = -1;
-    int cur_lg = 5;
+    int cur_lg = 4;  // log2 buckets of the current table
     const int m = 1 << P.p;
 
     while (true) {
         unsigned long long e0 = 0;
         if (lane == 0) e0 = atomicAdd(P.work, (unsigned long long)P.chunk);
         e0 = __shfl_sync(FULL, e0, 0);
-        if (e0 >= (unsigned long long)P.n_edges) break;
-        const int64_t e1 = min((int64_t)e0 + P.chunk, P.n_edges);
+        if (e0 >= (unsigned long long)n_edges) break;
+        const int64_t e1 = min((int64_t)e0 + P.chunk, n_edges);
         for (int64_t eb = (int64_t)e0; eb < e1; eb += 32) {
             const int64_t e = eb + lane;
-            bool valid = e < e1;
             int32_t u = 0, v = 0, us = 0, ue = 0, vs = 0, ve = 0;
-            if (valid) {
-                u = __ldg(P.edge_u + e);
-                v = __ldg(P.edge_v + e);
-                if ((uint64_t)(uint32_t)u >= (uint64_t)P.n_nodes || (uint64_t)(uint32_t)v >= (uint64_t)P.n_nodes ||
-                    u < 0 || v < 0) {
-                    status |= ST_BAD_EDGE;
-                    valid = false;
-                }
-            }
-            if (valid) {
-                us = __ldg(row_ptr + u); ue = __ldg(row_ptr + u + 1);
-                vs = __ldg(row_ptr + v); ve = __ldg(row_ptr + v + 1);
-                if (us < 0 || ue < us || (int64_t)ue > P.nnz || vs < 0 || ve < vs || (int64_t)ve > P.nnz) {
-                    status |= ST_BAD_ROW;
-                    valid = false;
-                }
-            }
+            bool valid = e < e1 && load_edge(P, e, u, v, us, ue, vs, ve, status);
             bool is_hll = false;
             int64_t slot_u = -1, slot_v = -1;
             int32_t du = 0, dv = 0;
             if (MODE != MODE_EXACT && valid) {
-                du = __ldg(P.degrees + u);
-                dv = __ldg(P.degrees + v);
-                const int64_t proxy = du < dv ? du : dv;
-                const bool wants = proxy >= P.gamma;
-                if (P.slot) {
-                    slot_u = __ldg(P.slot + u);
-                    slot_v = __ldg(P.slot + v);
-                } else {
-                    slot_u = __ldg(P.has + u) == 1 ? (int64_t)u : -1;
-                    slot_v = __ldg(P.has + v) == 1 ? (int64_t)v : -1;
-                }
-                if (slot_u >= P.n_rows || slot_v >= P.n_rows) { status |= ST_BAD_SLOT; valid = false; }
-                const bool both = slot_u >= 0 && slot_v >= 0;
+                bool wants, both;
+                valid = route(P, u, v, du, dv, slot_u, slot_v, wants, both, status);
                 is_hll = valid && wants && both;
-                if (MODE != MODE_HYB_HLL && valid && wants && !both) ++n_fallback;
+                // n_fallback: counted by the fused launch and, in split mode,
+                // by the HLL launch (which sees every edge in both variants)
+                if (MODE != MODE_HYB_EXACT && valid && wants && !both) ++n_fallback;
             }
             const bool do_exact = valid && !is_hll && MODE != MODE_HYB_HLL;
             const bool do_hll = valid && is_hll && MODE != MODE_HYB_EXACT;
@@ -192,7 +300,7 @@ __global__ void __launch_bounds__(256, 1) count_kernel(const CountParams P) {
             const int lu = ue - us, lv = ve - vs;
             const bool tiny = do_exact && (lu + lv <= P.tiny || lu == 0 || lv == 0);
             if (tiny) {
-                uint32_t c = (lu && lv) ? lane_merge_count(col_idx + us, lu, col_idx + vs, lv) : 0u;
+                const uint32_t c = (lu && lv) ? lane_merge_count(col_idx + us, lu, col_idx + vs, lv) : 0u;
                 acc += c;
                 if (DETAILS) P.pe_support[e] = c;
             }
@@ -206,17 +314,17 @@ __global__ void __launch_bounds__(256, 1) count_kernel(const CountParams P) {
                 const int32_t gdu = __shfl_sync(FULL, lu, lead);
                 const bool in = (grp >> lane) & 1u;
                 if (gdu > cap_keys) {
-                    // row too long for a warp table: binary search per edge
+                    // table side too long for a warp table: binary search per edge
                     unsigned g = grp;
                     while (g) {
                         const int j = __ffs(g) - 1;
                         g &= g - 1;
                         const int32_t jvs = __shfl_sync(FULL, vs, j);
                         const int32_t jlv = __shfl_sync(FULL, lv, j);
-                        uint32_t c = warp_bsearch_count(col_idx + gus, gdu, col_idx + jvs, jlv, lane);
+                        const uint32_t c = warp_bsearch_count(col_idx + gus, gdu, col_idx + jvs, jlv, lane);
                         acc += c;
                         if (DETAILS) {
-                            uint32_t tot = (uint32_t)warp_sum_u64(c);
+                            const uint32_t tot = (uint32_t)warp_sum_u64(c);
                             const int64_t ej = __shfl_sync(FULL, e, j);
                             if (lane == 0) P.pe_support[ej] = tot;
                         }
@@ -224,28 +332,41 @@ __global__ void __launch_bounds__(256, 1) count_kernel(const CountParams P) {
                     continue;
                 }
                 if (ucur != cur_u) {
-                    // (re)build the warp's table for N+(ucur)
-                    int lg = ceil_log2_i(gdu) + 2;
-                    lg = lg < 5 ? 5 : (lg > cap_lg ? cap_lg : lg);
-                    const int sz = 1 << lg;
+                    // (re)build the warp's table for N+(ucur): 2^lgb buckets,
+                    // load gdu / 2^(lgb+1) <= 1/2
+                    int lgb = ceil_log2_i(gdu);
+                    lgb = lgb < 4 ? 4 : lgb;
+                    const int nslots = 2 << lgb;
                     __syncwarp();
-                    for (int i = lane; i < sz; i += 32) table[i] = -1;
+                    for (int i = lane; i < nslots; i += 32) table[i] = -1;
                     __syncwarp();
-                    const uint32_t mask = (uint32_t)sz - 1u;
-                    for (int i = lane; i < gdu; i += 32) {
-                        const int32_t x = __ldg(col_idx + gus + i);
-                        uint32_t h = tbl_hash(x, lg);
-                        while (true) {
-                            const int32_t old = atomicCAS(&table[h], -1, x);
-                            if (old == -1 || old == x) break;
-                            h = (h + 1u) & mask;
+                    bool ok = true;
+                    for (int i = lane; i < gdu; i += 32) ok &= tbl_insert(table, __ldg(col_idx + gus + i), lgb);
+                    __syncwarp();
+                    if (!__all_sync(FULL, ok)) {
+                        // cuckoo placement failed: binary search for this group
+                        cur_u = -1;
+                        unsigned g = grp;
+                        while (g) {
+                            const int j = __ffs(g) - 1;
+                            g &= g - 1;
+                            const int32_t jvs = __shfl_sync(FULL, vs, j);
+                            const int32_t jlv = __shfl_sync(FULL, lv, j);
+                            const uint32_t c = warp_bsearch_count(col_idx + gus, gdu, col_idx + jvs, jlv, lane);
+                            acc += c;
+                            if (DETAILS) {
+                                const uint32_t tot = (uint32_t)warp_sum_u64(c);
+                                const int64_t ej = __shfl_sync(FULL, e, j);
+                                if (lane == 0) P.pe_support[ej] = tot;
+                            }
                         }
+                        continue;
                     }
-                    __syncwarp();
                     cur_u = ucur;
-                    cur_lg = lg;
+                    cur_lg = lgb;
                 }
-                // flatten the group's probe lists N+(v) into quads
+                const int2* T2 = reinterpret_cast<const int2*>(table);
+                // flatten the group's probe lists into quads
                 int q0, nq;
                 if (VEC) {
                     q0 = vs >> 2;
@@ -285,9 +406,9 @@ __global__ void __launch_bounds__(256, 1) count_kernel(const CountParams P) {
                     int64_t my_e = 0;
                     if (DETAILS) my_e = __shfl_sync(FULL, c_e, j);
                     const int t = T0 + lane;
+                    uint32_t c = 0;
                     if (t < W) {
                         const int qd = my_qb + t;
-                        uint32_t c = 0;
                         if (VEC) {
                             const int base = qd * 4;
                             int4 val;
@@ -299,16 +420,17 @@ __global__ void __launch_bounds__(256, 1) count_kernel(const CountParams P) {
                                 val.z = base + 2 < P.nnz ? __ldg(col_idx + base + 2) : -1;
                                 val.w = base + 3 < P.nnz ? __ldg(col_idx + base + 3) : -1;
                             }
-                            if (base + 0 >= my_vs && base + 0 < my_ve) c += tbl_probe(table, cur_lg, val.x);
-                            if (base + 1 >= my_vs && base + 1 < my_ve) c += tbl_probe(table, cur_lg, val.y);
-                            if (base + 2 >= my_vs && base + 2 < my_ve) c += tbl_probe(table, cur_lg, val.z);
-                            if (base + 3 >= my_vs && base + 3 < my_ve) c += tbl_probe(table, cur_lg, val.w);
+                            const int lo = my_vs - base, hi = my_ve - base;  // valid elements: [lo, hi)
+                            c += (0 >= lo && 0 < hi) ? tbl_lookup(T2, val.x, cur_lg) : 0u;
+                            c += (1 >= lo && 1 < hi) ? tbl_lookup(T2, val.y, cur_lg) : 0u;
+                            c += (2 >= lo && 2 < hi) ? tbl_lookup(T2, val.z, cur_lg) : 0u;
+                            c += (3 >= lo && 3 < hi) ? tbl_lookup(T2, val.w, cur_lg) : 0u;
                         } else {
-                            c = tbl_probe(table, cur_lg, __ldg(col_idx + qd));
+                            c = tbl_lookup(T2, __ldg(col_idx + qd), cur_lg);
                         }
-                        acc += c;
-                        if (DETAILS && c) atomicAdd((unsigned long long*)(P.pe_support + my_e), (unsigned long long)c);
                     }
+                    acc += c;
+                    if (DETAILS && c) atomicAdd((unsigned long long*)(P.pe_support + my_e), (unsigned long long)c);
                 }
             }
 
@@ -367,21 +489,21 @@ __global__ void __launch_bounds__(256, 1) count_kernel(const CountParams P) {
 }
 
 // ---------------------------------------------------------------- host ------
-static constexpr int kWarps = 8;
-static constexpr int kThreads = kWarps * 32;
-
 struct Tuning {
     int chunk = 64;
-    int slots_log2 = 11;  // 2048 slots = 8 KB per warp
+    int slots_log2 = 11;    // 2048 slots = 8 KB per warp
     int tiny = 16;
     int blocks_per_sm = 0;  // 0: occupancy maximum
+    int warps = 8;          // warps per CTA
+    int pairs = 1;          // table-side / probe-side reorientation
 };
 static Tuning g_tuning;
 
 template <int MODE, bool VEC, bool DETAILS>
 static int launch_mode(const CountParams& P, cudaStream_t st) {
     auto kern = count_kernel<MODE, VEC, DETAILS>;
-    const size_t smem = (size_t)kWarps * ((size_t)1 << P.slots_log2) * sizeof(int32_t);
+    const int threads = g_tuning.warps * 32;
+    const size_t smem = (size_t)g_tuning.warps * ((size_t)1 << P.slots_log2) * sizeof(int32_t);
     static size_t smem_set = 0;  // largest dynamic smem opted into so far
     cudaError_t e;
     if (smem > smem_set) {
@@ -391,12 +513,12 @@ static int launch_mode(const CountParams& P, cudaStream_t st) {
     }
     int bps = g_tuning.blocks_per_sm;
     if (bps <= 0) {
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, kThreads, smem);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, threads, smem);
         if (e != cudaSuccess) return cuda_status(e, "occupancy(count_kernel)");
         if (bps < 1) bps = 1;
     }
     const int grid = sm_count() * bps;
-    kern<<<grid, kThreads, smem, st>>>(P);
+    kern<<<grid, threads, smem, st>>>(P);
     TCHLL_CHECK_LAUNCH("count_kernel");
     return TCHLL_OK;
 }
@@ -408,31 +530,110 @@ static int launch_count(const CountParams& P, bool details, cudaStream_t st) {
     return vec ? launch_mode<MODE, true, false>(P, st) : launch_mode<MODE, false, false>(P, st);
 }
 
+struct CountWs {
+    unsigned long long* ctr;  // work counters
+    int32_t* cnt;             // n_nodes + 1 (histogram)
+    int32_t* off;             // n_nodes + 1 (scan, then scatter cursor)
+    int32_t* px;              // n_edges
+    int32_t* py;              // n_edges
+    void* tmp;
+    size_t tmp_bytes;
+};
+
+static bool carve_count(void* ws, size_t bytes, int64_t n_nodes, int64_t n_edges, CountWs& W, size_t* need) {
+    const size_t N = (size_t)(n_nodes > 0 ? n_nodes : 0) + 1;
+    const size_t E = (size_t)(n_edges > 0 ? n_edges : 1);
+    size_t tb = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tb, (int32_t*)nullptr, (int32_t*)nullptr, (int)N);
+    Carve cv(ws, bytes);
+    W.ctr = cv.take<unsigned long long>(4);
+    W.cnt = cv.take<int32_t>(N);
+    W.off = cv.take<int32_t>(N);
+    W.px = cv.take<int32_t>(E);
+    W.py = cv.take<int32_t>(E);
+    W.tmp_bytes = tb;
+    W.tmp = cv.take<char>(tb);
+    if (need) *need = cv.off;
+    return cv.ok();
+}
+
+static int grid_edges(int64_t n) {
+    int64_t g = (n + 255) / 256;
+    const int64_t cap = (int64_t)sm_count() * 16;
+    if (g > cap) g = cap;
+    return g < 1 ? 1 : (int)g;
+}
+
+// Build the grouped (x, y) pair list of the exact edges into Q.
+template <bool HYB>
+static int build_pairs(const CountParams& P, const CountWs& W, CountParams& Q, cudaStream_t st) {
+    const int64_t N = P.n_nodes + 1;
+    TCHLL_CUDA(cudaMemsetAsync(W.cnt, 0, sizeof(int32_t) * N, st));
+    const int g = grid_edges(P.n_edges);
+    pair_hist_kernel<HYB><<<g, 256, 0, st>>>(P, W.cnt);
+    TCHLL_CHECK_LAUNCH("pair_hist_kernel");
+    size_t tb = W.tmp_bytes;
+    TCHLL_CUDA(cub::DeviceScan::ExclusiveSum(W.tmp, tb, W.cnt, W.off, (int)N, st));
+    count_launch();
+    // W.off[n_nodes] is the number of pairs; the scatter advances off[x] for
+    // x < n_nodes only, so the total survives.
+    pair_scatter_kernel<HYB><<<g, 256, 0, st>>>(P, W.off, W.px, W.py);
+    TCHLL_CHECK_LAUNCH("pair_scatter_kernel");
+    Q = P;
+    Q.edge_u = W.px;
+    Q.edge_v = W.py;
+    Q.n_edges_dev = W.off + P.n_nodes;
+    return TCHLL_OK;
+}
+
 static int run_count(CountParams P, int mode, bool details, void* ws, size_t ws_bytes, cudaStream_t st) {
-    Carve cv(ws, ws_bytes);
-    unsigned long long* ctr = cv.take<unsigned long long>(2);
-    if (!cv.ok()) { set_error("workspace too small: need %zu bytes, have %zu", cv.off, ws_bytes); return TCHLL_EWORKSPACE; }
-    TCHLL_CUDA(cudaMemsetAsync(ctr, 0, 2 * sizeof(unsigned long long), st));
+    CountWs W;
+    size_t need = 0;
+    if (!carve_count(ws, ws_bytes, P.n_nodes, P.n_edges, W, &need) || ws == nullptr) {
+        set_error("workspace too small: need %zu bytes, have %zu", need, ws_bytes);
+        return TCHLL_EWORKSPACE;
+    }
+    TCHLL_CUDA(cudaMemsetAsync(W.ctr, 0, 4 * sizeof(unsigned long long), st));
     TCHLL_CUDA(cudaMemsetAsync(P.result, 0, sizeof(tchll_count_result), st));
     if (details && P.pe_support) TCHLL_CUDA(cudaMemsetAsync(P.pe_support, 0, sizeof(int64_t) * P.n_edges, st));
     if (details && P.pe_method) TCHLL_CUDA(cudaMemsetAsync(P.pe_method, 0, P.n_edges, st));
     P.chunk = g_tuning.chunk;
     P.slots_log2 = g_tuning.slots_log2;
     P.tiny = g_tuning.tiny;
+    P.n_edges_dev = nullptr;
     if (P.n_edges == 0) return TCHLL_OK;
+    const bool pairs = g_tuning.pairs && !details;
     int rc;
+    CountParams Q;
     switch (mode) {
         case MODE_EXACT:
-            P.work = ctr;
+            P.work = W.ctr;
+            if (pairs) {
+                rc = build_pairs<false>(P, W, Q, st);
+                if (rc) return rc;
+                return launch_count<MODE_EXACT>(Q, false, st);
+            }
             return launch_count<MODE_EXACT>(P, details, st);
-        case MODE_HYBRID:
-            P.work = ctr;
+        case MODE_HYBRID:  // one fused launch over the edges as given
+            P.work = W.ctr;
             return launch_count<MODE_HYBRID>(P, details, st);
         case 2:  // split: exact-routed edges, then HLL-routed edges
-            P.work = ctr;
+            if (pairs) {
+                // The pair launch adds the exact supports; the edge-wise
+                // HLL launch adds the HLL estimates and every routing count
+                // except n_exact, which the pair launch counts (one per pair).
+                P.work = W.ctr;
+                rc = build_pairs<true>(P, W, Q, st);
+                if (rc) return rc;
+                rc = launch_count<MODE_EXACT>(Q, false, st);
+                if (rc) return rc;
+                P.work = W.ctr + 1;
+                return launch_count<MODE_HYB_HLL>(P, false, st);
+            }
+            P.work = W.ctr;
             rc = launch_count<MODE_HYB_EXACT>(P, details, st);
             if (rc) return rc;
-            P.work = ctr + 1;
+            P.work = W.ctr + 1;
             return launch_count<MODE_HYB_HLL>(P, details, st);
         default:
             set_error("unknown count mode %d", mode);
@@ -443,7 +644,8 @@ static int run_count(CountParams P, int mode, bool details, void* ws, size_t ws_
 static int check_common(const int32_t* row_ptr, int64_t n_nodes, const int32_t* col_idx, int64_t nnz,
                         const int32_t* eu, const int32_t* ev, int64_t n_edges, tchll_count_result* result) {
     TCHLL_ARG(n_nodes >= 0 && nnz >= 0 && n_edges >= 0, "negative size");
-    TCHLL_ARG(n_nodes < (int64_t)INT32_MAX && nnz <= (int64_t)INT32_MAX, "int32 CSR limits exceeded");
+    TCHLL_ARG(n_nodes < (int64_t)INT32_MAX && nnz <= (int64_t)INT32_MAX && n_edges <= (int64_t)INT32_MAX,
+              "int32 CSR limits exceeded");
     TCHLL_ARG(result != nullptr, "result pointer is null");
     TCHLL_ARG(n_edges == 0 || (eu && ev && row_ptr), "null edge or row_ptr pointer");
     TCHLL_ARG(nnz == 0 || col_idx, "null col_idx");
@@ -454,12 +656,10 @@ static int check_common(const int32_t* row_ptr, int64_t n_nodes, const int32_t* 
 
 using namespace tchll;
 
-TCHLL_EXPORT int tchll_count_workspace_bytes(int64_t n_edges, size_t* bytes) {
-    (void)n_edges;
-    if (!bytes) { set_error("bytes is null"); return TCHLL_EINVAL; }
-    Carve cv(nullptr, 0);
-    cv.take<unsigned long long>(2);
-    *bytes = cv.off;
+TCHLL_EXPORT int tchll_count_workspace_bytes(int64_t n_nodes, int64_t n_edges, size_t* bytes) {
+    TCHLL_ARG(bytes != nullptr && n_nodes >= 0 && n_edges >= 0, "bad arguments");
+    CountWs W;
+    carve_count(nullptr, 0, n_nodes, n_edges, W, bytes);
     return TCHLL_OK;
 }
 
@@ -470,8 +670,13 @@ TCHLL_EXPORT int tchll_exact_count(const int32_t* row_ptr, int64_t n_nodes, cons
     int rc = check_common(row_ptr, n_nodes, col_idx, nnz, edge_u, edge_v, n_edges, result);
     if (rc) return rc;
     CountParams P{};
-    P.row_ptr = row_ptr; P.n_nodes = n_nodes; P.col_idx = col_idx; P.nnz = nnz;
-    P.edge_u = edge_u; P.edge_v = edge_v; P.n_edges = n_edges;
+    P.row_ptr = row_ptr;
+    P.n_nodes = n_nodes;
+    P.col_idx = col_idx;
+    P.nnz = nnz;
+    P.edge_u = edge_u;
+    P.edge_v = edge_v;
+    P.n_edges = n_edges;
     P.pe_support = per_edge_support;
     P.result = result;
     P.p = 4;
@@ -486,7 +691,6 @@ static int hybrid_common(const int32_t* row_ptr, int64_t n_nodes, const int32_t*
     int rc = check_common(row_ptr, n_nodes, col_idx, nnz, edge_u, edge_v, n_edges, result);
     if (rc) return rc;
     TCHLL_ARG(p >= 4 && p <= 16, "p must be in [4, 16], got %d", p);
-    TCHLL_ARG(mode >= 1 && mode <= 2, "mode must be 1 (fused) or 2 (split), got %d", mode);
     TCHLL_ARG(n_edges == 0 || degrees, "degrees is null");
     TCHLL_ARG(n_rows == 0 || regs, "register rows are null");
     TCHLL_ARG(slot || has || n_edges == 0, "need slot (compact) or has_sketch (dense)");
@@ -494,13 +698,26 @@ static int hybrid_common(const int32_t* row_ptr, int64_t n_nodes, const int32_t*
     TCHLL_ARG(!details || (pe_support && pe_s_hat && pe_s_cl && pe_method),
               "per-edge outputs must be all set or all null");
     CountParams P{};
-    P.row_ptr = row_ptr; P.n_nodes = n_nodes; P.col_idx = col_idx; P.nnz = nnz;
-    P.edge_u = edge_u; P.edge_v = edge_v; P.n_edges = n_edges;
-    P.degrees = degrees; P.regs = regs; P.n_rows = n_rows; P.slot = slot; P.has = has;
-    P.p = p; P.gamma = gamma;
-    P.pe_support = pe_support; P.pe_s_hat = pe_s_hat; P.pe_s_cl = pe_s_cl; P.pe_method = pe_method;
+    P.row_ptr = row_ptr;
+    P.n_nodes = n_nodes;
+    P.col_idx = col_idx;
+    P.nnz = nnz;
+    P.edge_u = edge_u;
+    P.edge_v = edge_v;
+    P.n_edges = n_edges;
+    P.degrees = degrees;
+    P.regs = regs;
+    P.n_rows = n_rows;
+    P.slot = slot;
+    P.has = has;
+    P.p = p;
+    P.gamma = gamma;
+    P.pe_support = pe_support;
+    P.pe_s_hat = pe_s_hat;
+    P.pe_s_cl = pe_s_cl;
+    P.pe_method = pe_method;
     P.result = result;
-    return run_count(P, mode == 1 ? MODE_HYBRID : 2, details, ws, wsb, (cudaStream_t)stream);
+    return run_count(P, mode, details, ws, wsb, (cudaStream_t)stream);
 }
 
 TCHLL_EXPORT int tchll_hybrid_count_dense(const int32_t* row_ptr, int64_t n_nodes, const int32_t* col_idx,
@@ -509,9 +726,9 @@ TCHLL_EXPORT int tchll_hybrid_count_dense(const int32_t* row_ptr, int64_t n_node
                                           const uint8_t* has_sketch, int32_t p, int64_t gamma,
                                           int32_t split_kernels, tchll_count_result* result, void* workspace,
                                           size_t workspace_bytes, void* stream) {
-    return hybrid_common(row_ptr, n_nodes, col_idx, nnz, edge_u, edge_v, n_edges, degrees, sketch_regs,
-                         n_nodes, nullptr, has_sketch, p, gamma, split_kernels ? 2 : 1, nullptr, nullptr,
-                         nullptr, nullptr, result, workspace, workspace_bytes, stream);
+    return hybrid_common(row_ptr, n_nodes, col_idx, nnz, edge_u, edge_v, n_edges, degrees, sketch_regs, n_nodes,
+                         nullptr, has_sketch, p, gamma, split_kernels ? 2 : MODE_HYBRID, nullptr, nullptr, nullptr,
+                         nullptr, result, workspace, workspace_bytes, stream);
 }
 
 TCHLL_EXPORT int tchll_hybrid_count_compact(const int32_t* row_ptr, int64_t n_nodes, const int32_t* col_idx,
@@ -524,15 +741,16 @@ TCHLL_EXPORT int tchll_hybrid_count_compact(const int32_t* row_ptr, int64_t n_no
                                             void* workspace, size_t workspace_bytes, void* stream) {
     TCHLL_ARG(slot != nullptr || n_edges == 0, "slot is null");
     return hybrid_common(row_ptr, n_nodes, col_idx, nnz, edge_u, edge_v, n_edges, degrees, rows, n_rows, slot,
-                         nullptr, p, gamma, split_kernels ? 2 : 1, per_edge_support, per_edge_s_hat,
+                         nullptr, p, gamma, split_kernels ? 2 : MODE_HYBRID, per_edge_support, per_edge_s_hat,
                          per_edge_s_clamped, per_edge_method, result, workspace, workspace_bytes, stream);
 }
 
 TCHLL_EXPORT int tchll_set_count_tuning(int32_t chunk, int32_t slots_log2, int32_t tiny, int32_t blocks_per_sm) {
     TCHLL_ARG(chunk >= 32 && chunk % 32 == 0 && chunk <= (1 << 20), "chunk must be a multiple of 32 in [32, 2^20]");
-    TCHLL_ARG(slots_log2 >= 6 && slots_log2 <= 13, "slots_log2 must be in [6, 13]");
     TCHLL_ARG(tiny >= 0 && tiny <= 4096, "tiny must be in [0, 4096]");
     TCHLL_ARG(blocks_per_sm >= 0 && blocks_per_sm <= 32, "blocks_per_sm must be in [0, 32]");
+    TCHLL_ARG(slots_log2 >= 6 && slots_log2 <= 15 && (size_t)g_tuning.warps * ((size_t)4 << slots_log2) <= 227 * 1024,
+              "slots_log2 must be in [6, 15] with warps x 2^slots_log2 x 4 bytes within 227 KB of shared memory");
     g_tuning.chunk = chunk;
     g_tuning.slots_log2 = slots_log2;
     g_tuning.tiny = tiny;
@@ -540,11 +758,22 @@ TCHLL_EXPORT int tchll_set_count_tuning(int32_t chunk, int32_t slots_log2, int32
     return TCHLL_OK;
 }
 
-TCHLL_EXPORT int tchll_get_count_tuning(int32_t* out4) {
-    TCHLL_ARG(out4 != nullptr, "out is null");
-    out4[0] = g_tuning.chunk;
-    out4[1] = g_tuning.slots_log2;
-    out4[2] = g_tuning.tiny;
-    out4[3] = g_tuning.blocks_per_sm;
+TCHLL_EXPORT int tchll_set_count_shape(int32_t warps_per_cta, int32_t pairs) {
+    TCHLL_ARG(warps_per_cta >= 1 && warps_per_cta <= 8, "warps_per_cta must be in [1, 8]");
+    TCHLL_ARG((size_t)warps_per_cta * ((size_t)4 << g_tuning.slots_log2) <= 227 * 1024,
+              "warps x 2^slots_log2 x 4 bytes must fit 227 KB of shared memory");
+    g_tuning.warps = warps_per_cta;
+    g_tuning.pairs = pairs ? 1 : 0;
+    return TCHLL_OK;
+}
+
+TCHLL_EXPORT int tchll_get_count_tuning(int32_t* out6) {
+    TCHLL_ARG(out6 != nullptr, "out is null");
+    out6[0] = g_tuning.chunk;
+    out6[1] = g_tuning.slots_log2;
+    out6[2] = g_tuning.tiny;
+    out6[3] = g_tuning.blocks_per_sm;
+    out6[4] = g_tuning.warps;
+    out6[5] = g_tuning.pairs;
     return TCHLL_OK;
 }
