@@ -130,6 +130,15 @@ int tchll_set_count_tuning(int32_t chunk, int32_t slots_log2, int32_t tiny, int3
 int tchll_set_count_shape(int32_t warps_per_cta, int32_t pairs);
 int tchll_get_count_tuning(int32_t* out6 /* host */);
 
+/* Phase timing for measurement (process-wide host state, off by default).
+ * When enabled, the counting entry points record CUDA events on the
+ * caller's stream around their phases; tchll_phase_times then waits for the
+ * last call's events and writes milliseconds: ms3[0] pair regrouping,
+ * ms3[1] exact-count kernel, ms3[2] HLL kernel (-1 for a phase the call did
+ * not run). */
+int tchll_set_phase_timing(int32_t enable);
+int tchll_phase_times(float* ms3 /* host */);
+
 /* ------------------------------------------------------------ sketches --- */
 /*
  * Dense sketch build, launch-compatible with build_sketches_kernel

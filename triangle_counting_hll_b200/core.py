@@ -260,6 +260,19 @@ def get_count_tuning() -> dict:
             "pairs": out[5]}
 
 
+def set_phase_timing(enable: bool) -> None:
+    check(load().tchll_set_phase_timing(1 if enable else 0))
+
+
+def phase_times() -> dict:
+    """Milliseconds of the last counting call's phases (needs
+    set_phase_timing(True) before the call); None for phases not run."""
+    out = (C.c_float * 3)()
+    check(load().tchll_phase_times(C.cast(out, C.c_void_p)))
+    names = ("pairs", "count", "hll")
+    return {n: (float(v) if v >= 0 else None) for n, v in zip(names, out)}
+
+
 # ----------------------------------------------------------- sketches (a4)
 def build_sketches_dense_tensors(row_ptr, col_idx, n_nodes: int, theta: int, p: int, sketch_regs,
                                  has_sketch) -> None:

@@ -394,43 +394,73 @@ __global__ void __launch_bounds__(256, 1) count_kernel(const CountParams P) {
                 const int excl = incl - c_nq;
                 const int W = __shfl_sync(FULL, incl, 31);
                 const int qb = c_q0 - excl;
-                for (int T0 = 0; T0 < W; T0 += 32) {
-                    const unsigned cover = __ballot_sync(FULL, lane < k && excl <= T0 && T0 < incl);
-                    const int b = __ffs(cover) - 1;
-                    const unsigned bit = (lane < k && excl > T0 && excl < T0 + 32) ? (1u << (excl - T0)) : 0u;
-                    const unsigned B = __reduce_or_sync(FULL, bit);
-                    const int j = (b + __popc(B & ((2u << lane) - 1u))) & 31;
-                    const int my_qb = __shfl_sync(FULL, qb, j);
-                    const int32_t my_vs = __shfl_sync(FULL, c_vs, j);
-                    const int32_t my_ve = __shfl_sync(FULL, c_ve, j);
-                    int64_t my_e = 0;
-                    if (DETAILS) my_e = __shfl_sync(FULL, c_e, j);
-                    const int t = T0 + lane;
-                    uint32_t c = 0;
-                    if (t < W) {
-                        const int qd = my_qb + t;
-                        if (VEC) {
-                            const int base = qd * 4;
-                            int4 val;
-                            if ((int64_t)base + 3 < P.nnz) {
-                                val = __ldg(reinterpret_cast<const int4*>(col_idx) + qd);
-                            } else {
-                                val.x = base + 0 < P.nnz ? __ldg(col_idx + base + 0) : -1;
-                                val.y = base + 1 < P.nnz ? __ldg(col_idx + base + 1) : -1;
-                                val.z = base + 2 < P.nnz ? __ldg(col_idx + base + 2) : -1;
-                                val.w = base + 3 < P.nnz ? __ldg(col_idx + base + 3) : -1;
+                // Windows of 32 quads; UNR windows are mapped, loaded and then
+                // probed together so each lane has UNR 16-byte loads in flight.
+                constexpr int UNR = VEC ? 4 : 2;
+                for (int T0 = 0; T0 < W; T0 += 32 * UNR) {
+                    int qd[UNR], lo[UNR], hi[UNR];
+                    int64_t my_e[UNR];
+#pragma unroll
+                    for (int i = 0; i < UNR; ++i) {
+                        const int Ti = T0 + 32 * i;
+                        qd[i] = -1;
+                        lo[i] = hi[i] = 0;
+                        my_e[i] = 0;
+                        if (Ti < W) {  // warp-uniform
+                            const unsigned cover = __ballot_sync(FULL, lane < k && excl <= Ti && Ti < incl);
+                            const int b = __ffs(cover) - 1;
+                            const unsigned bit =
+                                (lane < k && excl > Ti && excl < Ti + 32) ? (1u << (excl - Ti)) : 0u;
+                            const unsigned B = __reduce_or_sync(FULL, bit);
+                            const int j = (b + __popc(B & ((2u << lane) - 1u))) & 31;
+                            const int my_qb = __shfl_sync(FULL, qb, j);
+                            const int32_t my_vs = __shfl_sync(FULL, c_vs, j);
+                            const int32_t my_ve = __shfl_sync(FULL, c_ve, j);
+                            if (DETAILS) my_e[i] = __shfl_sync(FULL, c_e, j);
+                            if (Ti + lane < W) {
+                                qd[i] = my_qb + Ti + lane;
+                                const int base = VEC ? qd[i] * 4 : qd[i];
+                                lo[i] = my_vs - base;  // valid elements of the quad: [lo, hi)
+                                hi[i] = my_ve - base;
                             }
-                            const int lo = my_vs - base, hi = my_ve - base;  // valid elements: [lo, hi)
-                            c += (0 >= lo && 0 < hi) ? tbl_lookup(T2, val.x, cur_lg) : 0u;
-                            c += (1 >= lo && 1 < hi) ? tbl_lookup(T2, val.y, cur_lg) : 0u;
-                            c += (2 >= lo && 2 < hi) ? tbl_lookup(T2, val.z, cur_lg) : 0u;
-                            c += (3 >= lo && 3 < hi) ? tbl_lookup(T2, val.w, cur_lg) : 0u;
-                        } else {
-                            c = tbl_lookup(T2, __ldg(col_idx + qd), cur_lg);
                         }
                     }
-                    acc += c;
-                    if (DETAILS && c) atomicAdd((unsigned long long*)(P.pe_support + my_e), (unsigned long long)c);
+                    int4 val[UNR];
+#pragma unroll
+                    for (int i = 0; i < UNR; ++i) {
+                        val[i] = make_int4(-1, -1, -1, -1);
+                        if (qd[i] >= 0) {
+                            if (VEC) {
+                                const int base = qd[i] * 4;
+                                if ((int64_t)base + 3 < P.nnz) {
+                                    val[i] = __ldg(reinterpret_cast<const int4*>(col_idx) + qd[i]);
+                                } else {
+                                    val[i].x = base + 0 < P.nnz ? __ldg(col_idx + base + 0) : -1;
+                                    val[i].y = base + 1 < P.nnz ? __ldg(col_idx + base + 1) : -1;
+                                    val[i].z = base + 2 < P.nnz ? __ldg(col_idx + base + 2) : -1;
+                                    val[i].w = base + 3 < P.nnz ? __ldg(col_idx + base + 3) : -1;
+                                }
+                            } else {
+                                val[i].x = __ldg(col_idx + qd[i]);
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int i = 0; i < UNR; ++i) {
+                        if (qd[i] < 0) continue;
+                        uint32_t c = 0;
+                        if (VEC) {
+                            c += (0 >= lo[i] && 0 < hi[i]) ? tbl_lookup(T2, val[i].x, cur_lg) : 0u;
+                            c += (1 >= lo[i] && 1 < hi[i]) ? tbl_lookup(T2, val[i].y, cur_lg) : 0u;
+                            c += (2 >= lo[i] && 2 < hi[i]) ? tbl_lookup(T2, val[i].z, cur_lg) : 0u;
+                            c += (3 >= lo[i] && 3 < hi[i]) ? tbl_lookup(T2, val[i].w, cur_lg) : 0u;
+                        } else {
+                            c = tbl_lookup(T2, val[i].x, cur_lg);
+                        }
+                        acc += c;
+                        if (DETAILS && c)
+                            atomicAdd((unsigned long long*)(P.pe_support + my_e[i]), (unsigned long long)c);
+                    }
                 }
             }
 
@@ -498,6 +528,23 @@ struct Tuning {
     int pairs = 1;          // table-side / probe-side reorientation
 };
 static Tuning g_tuning;
+
+// Optional phase timing: CUDA events recorded on the caller's stream around
+// the pair regrouping, the exact-count launch and the HLL launch.
+struct PhaseTimer {
+    bool on = false;
+    bool made = false;
+    cudaEvent_t ev[4];
+    bool used[3] = {false, false, false};
+};
+static PhaseTimer g_phase;
+
+static void phase_mark(int i, cudaStream_t st) {
+    if (g_phase.on && g_phase.made) cudaEventRecord(g_phase.ev[i], st);
+}
+static void phase_reset() {
+    for (int i = 0; i < 3; ++i) g_phase.used[i] = false;
+}
 
 template <int MODE, bool VEC, bool DETAILS>
 static int launch_mode(const CountParams& P, cudaStream_t st) {
@@ -605,36 +652,61 @@ static int run_count(CountParams P, int mode, bool details, void* ws, size_t ws_
     const bool pairs = g_tuning.pairs && !details;
     int rc;
     CountParams Q;
+    phase_reset();
     switch (mode) {
         case MODE_EXACT:
             P.work = W.ctr;
             if (pairs) {
+                phase_mark(0, st);
                 rc = build_pairs<false>(P, W, Q, st);
                 if (rc) return rc;
-                return launch_count<MODE_EXACT>(Q, false, st);
+                phase_mark(1, st);
+                rc = launch_count<MODE_EXACT>(Q, false, st);
+                phase_mark(2, st);
+                g_phase.used[0] = g_phase.used[1] = true;
+                return rc;
             }
-            return launch_count<MODE_EXACT>(P, details, st);
+            phase_mark(1, st);
+            rc = launch_count<MODE_EXACT>(P, details, st);
+            phase_mark(2, st);
+            g_phase.used[1] = true;
+            return rc;
         case MODE_HYBRID:  // one fused launch over the edges as given
             P.work = W.ctr;
-            return launch_count<MODE_HYBRID>(P, details, st);
+            phase_mark(1, st);
+            rc = launch_count<MODE_HYBRID>(P, details, st);
+            phase_mark(2, st);
+            g_phase.used[1] = true;
+            return rc;
         case 2:  // split: exact-routed edges, then HLL-routed edges
             if (pairs) {
-                // The pair launch adds the exact supports; the edge-wise
-                // HLL launch adds the HLL estimates and every routing count
-                // except n_exact, which the pair launch counts (one per pair).
+                // The pair launch adds the exact supports and counts n_exact;
+                // the edge-wise HLL launch adds the HLL estimates, n_approx,
+                // n_clamped and n_fallback.
                 P.work = W.ctr;
+                phase_mark(0, st);
                 rc = build_pairs<true>(P, W, Q, st);
                 if (rc) return rc;
+                phase_mark(1, st);
                 rc = launch_count<MODE_EXACT>(Q, false, st);
                 if (rc) return rc;
+                phase_mark(2, st);
                 P.work = W.ctr + 1;
-                return launch_count<MODE_HYB_HLL>(P, false, st);
+                rc = launch_count<MODE_HYB_HLL>(P, false, st);
+                phase_mark(3, st);
+                g_phase.used[0] = g_phase.used[1] = g_phase.used[2] = true;
+                return rc;
             }
             P.work = W.ctr;
+            phase_mark(1, st);
             rc = launch_count<MODE_HYB_EXACT>(P, details, st);
             if (rc) return rc;
+            phase_mark(2, st);
             P.work = W.ctr + 1;
-            return launch_count<MODE_HYB_HLL>(P, details, st);
+            rc = launch_count<MODE_HYB_HLL>(P, details, st);
+            phase_mark(3, st);
+            g_phase.used[1] = g_phase.used[2] = true;
+            return rc;
         default:
             set_error("unknown count mode %d", mode);
             return TCHLL_EINVAL;
@@ -775,5 +847,27 @@ TCHLL_EXPORT int tchll_get_count_tuning(int32_t* out6) {
     out6[3] = g_tuning.blocks_per_sm;
     out6[4] = g_tuning.warps;
     out6[5] = g_tuning.pairs;
+    return TCHLL_OK;
+}
+
+TCHLL_EXPORT int tchll_set_phase_timing(int32_t enable) {
+    if (enable && !g_phase.made) {
+        for (int i = 0; i < 4; ++i) TCHLL_CUDA(cudaEventCreate(&g_phase.ev[i]));
+        g_phase.made = true;
+    }
+    g_phase.on = enable != 0;
+    phase_reset();
+    return TCHLL_OK;
+}
+
+TCHLL_EXPORT int tchll_phase_times(float* ms3) {
+    TCHLL_ARG(ms3 != nullptr, "out is null");
+    for (int i = 0; i < 3; ++i) ms3[i] = -1.0f;
+    if (!g_phase.on || !g_phase.made) return TCHLL_OK;
+    for (int i = 0; i < 3; ++i) {
+        if (!g_phase.used[i]) continue;
+        TCHLL_CUDA(cudaEventSynchronize(g_phase.ev[i + 1]));
+        TCHLL_CUDA(cudaEventElapsedTime(&ms3[i], g_phase.ev[i], g_phase.ev[i + 1]));
+    }
     return TCHLL_OK;
 }
