@@ -130,6 +130,25 @@ int tchll_set_count_tuning(int32_t chunk, int32_t slots_log2, int32_t tiny, int3
 int tchll_set_count_shape(int32_t warps_per_cta, int32_t pairs);
 int tchll_get_count_tuning(int32_t* out6 /* host */);
 
+/*
+ * Allocation-free exact count, for callers that cannot allocate device memory
+ * (a binding with no CUDA allocator of its own, or a service whose device
+ * memory is all reserved up front).  No counterpart in the reference.  Same
+ * result as tchll_exact_count without per-edge output, but the scratch comes
+ * from a fixed array of TCHLL_NOALLOC_SCRATCH_BYTES inside the library that
+ * every GPU loading the library reserves until the process exits; graphs
+ * needing more scratch (8 bytes per edge + 8 per vertex, so roughly
+ * n_nodes + n_edges <= 4 million) are rejected with TCHLL_EINVAL.  The first
+ * call on a device looks up the array's device address; make that first call
+ * before any stream capture.  All calls share the one array: calls that
+ * overlap on the GPU (different streams or devices sharing a context) race;
+ * serialize them.  Nothing here calls cudaMalloc or cudaFree.
+ */
+#define TCHLL_NOALLOC_SCRATCH_BYTES (32u << 20)
+int tchll_exact_count_noalloc(const int32_t* row_ptr, int64_t n_nodes, const int32_t* col_idx, int64_t nnz,
+                              const int32_t* edge_u, const int32_t* edge_v, int64_t n_edges,
+                              tchll_count_result* result, void* stream);
+
 /* Phase timing for measurement (process-wide host state, off by default).
  * When enabled, the counting entry points record CUDA events on the
  * caller's stream around their phases; tchll_phase_times then waits for the

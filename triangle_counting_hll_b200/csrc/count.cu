@@ -38,6 +38,8 @@
 //     on scheduling or partitioning: they are bit-identical run to run.
 #include <cub/cub.cuh>
 
+#include <mutex>
+
 #include "common.cuh"
 #include "hll_device.cuh"
 
@@ -870,4 +872,71 @@ TCHLL_EXPORT int tchll_phase_times(float* ms3) {
         TCHLL_CUDA(cudaEventElapsedTime(&ms3[i], g_phase.ev[i], g_phase.ev[i + 1]));
     }
     return TCHLL_OK;
+}
+
+// ------------------------------------------------ allocation-free variant ---
+// Some callers hold device pointers to a graph but cannot allocate device
+// memory themselves: a language binding without its own CUDA allocator, or a
+// service that hands all device memory to one arena up front and forbids
+// allocation on the request path.  tchll_exact_count_noalloc serves them with
+// the same exact count, taking its scratch (the pair list, histogram and work
+// counters) from this fixed array instead of a caller workspace.  Every GPU
+// that loads the library reserves the array until the process exits.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[TCHLL_NOALLOC_SCRATCH_BYTES];
+
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_ptr[256];  // device address of the array, per device
+
+// Host code must not pass g_noalloc_scratch itself to a kernel (on the host
+// the name stands for a host-side shadow, not the device array): look the
+// device address up once per device, with that device current.
+static int noalloc_scratch_ptr(void** out) {
+    int dev = -1;
+    TCHLL_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 256) {
+        set_error("device ordinal %d out of range", dev);
+        return TCHLL_EINVAL;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (g_noalloc_ptr[dev] == nullptr) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_status(e, "cudaGetSymbolAddress(noalloc scratch)");
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return TCHLL_OK;
+}
+
+TCHLL_EXPORT int tchll_exact_count_noalloc(const int32_t* row_ptr, int64_t n_nodes, const int32_t* col_idx,
+                                           int64_t nnz, const int32_t* edge_u, const int32_t* edge_v,
+                                           int64_t n_edges, tchll_count_result* result, void* stream) {
+    int rc = check_common(row_ptr, n_nodes, col_idx, nnz, edge_u, edge_v, n_edges, result);
+    if (rc) return rc;
+    CountWs W;
+    size_t need = 0;
+    carve_count(nullptr, 0, n_nodes, n_edges, W, &need);
+    if (need > (size_t)TCHLL_NOALLOC_SCRATCH_BYTES) {
+        set_error("graph too large for tchll_exact_count_noalloc: needs %zu bytes of scratch (8 per edge + 8 per "
+                  "vertex), the fixed limit is %u bytes; use tchll_exact_count with a workspace",
+                  need, (unsigned)TCHLL_NOALLOC_SCRATCH_BYTES);
+        return TCHLL_EINVAL;
+    }
+    void* scratch = nullptr;
+    rc = noalloc_scratch_ptr(&scratch);
+    if (rc) return rc;
+    CountParams P{};
+    P.row_ptr = row_ptr;
+    P.n_nodes = n_nodes;
+    P.col_idx = col_idx;
+    P.nnz = nnz;
+    P.edge_u = edge_u;
+    P.edge_v = edge_v;
+    P.n_edges = n_edges;
+    P.result = result;
+    P.p = 4;
+    // run_count clears the work counters, histogram and result on the stream
+    // before any kernel reads them, so leftovers of the previous call are
+    // harmless; calls that overlap on the GPU would share the array and race.
+    return run_count(P, MODE_EXACT, false, scratch, TCHLL_NOALLOC_SCRATCH_BYTES, (cudaStream_t)stream);
 }
