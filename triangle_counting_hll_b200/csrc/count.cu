@@ -108,21 +108,23 @@ __device__ __forceinline__ uint32_t tbl_lookup(const int2* T, int32_t x, int lgb
 // key could not be placed within the kick budget (the caller then falls back
 // to binary search for this table side).
 __device__ __forceinline__ bool tbl_insert(int32_t* T, int32_t x, int lgb) {
+    const Buckets xb = tbl_buckets(x, lgb);
+    if (atomicCAS(T + 2 * xb.b1, -1, x) == -1) return true;
+    if (atomicCAS(T + 2 * xb.b1 + 1, -1, x) == -1) return true;
+    if (atomicCAS(T + 2 * xb.b2, -1, x) == -1) return true;
+    if (atomicCAS(T + 2 * xb.b2 + 1, -1, x) == -1) return true;
+    // Both buckets full: cuckoo walk.  Take a slot of bucket b, move its
+    // resident to the resident's other bucket, and repeat there.  Slots never
+    // return to empty, so every evicted value is a real key.
     int32_t cur = x;
-    uint32_t b = tbl_buckets(cur, lgb).b1;
-    for (int kick = 0; kick < 96; ++kick) {
-        if (atomicCAS(T + 2 * b, -1, cur) == -1) return true;
-        if (atomicCAS(T + 2 * b + 1, -1, cur) == -1) return true;
-        const Buckets cb = tbl_buckets(cur, lgb);
-        const uint32_t alt = (b == cb.b1) ? cb.b2 : cb.b1;
-        if (atomicCAS(T + 2 * alt, -1, cur) == -1) return true;
-        if (atomicCAS(T + 2 * alt + 1, -1, cur) == -1) return true;
-        // both buckets full: evict a resident of alt and move it to its
-        // other bucket (slots never return to empty, so victim >= 0)
-        const int32_t victim = atomicExch(T + 2 * alt + (kick & 1), cur);
+    uint32_t b = (x & 1) ? xb.b2 : xb.b1;
+    for (int kick = 0; kick < 128; ++kick) {
+        const int32_t victim = atomicExch(T + 2 * b + ((kick >> 1) & 1), cur);
         cur = victim;
         const Buckets vb = tbl_buckets(cur, lgb);
-        b = (alt == vb.b1) ? vb.b2 : vb.b1;
+        b = (b == vb.b1) ? vb.b2 : vb.b1;
+        if (atomicCAS(T + 2 * b, -1, cur) == -1) return true;
+        if (atomicCAS(T + 2 * b + 1, -1, cur) == -1) return true;
     }
     return false;
 }
