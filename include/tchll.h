@@ -123,12 +123,14 @@ int tchll_hybrid_count_compact(const int32_t* row_ptr, int64_t n_nodes, const in
  * slots_log2: per-warp hash table capacity; tiny: lane-local merge threshold
  * on |N+u|+|N+v|; blocks_per_sm: 0 = occupancy maximum; warps_per_cta: 1-8;
  * pairs: 1 = probe the shorter list into a table of the longer one (edges
- * regrouped by a device counting sort), 0 = edges as given.  out6 receives
- * chunk, slots_log2, tiny, blocks_per_sm, warps_per_cta, pairs.  Results are
- * identical for every setting. */
+ * regrouped by a device counting sort), 0 = edges as given; sparse: 1 = hash
+ * tables at load <= 1/4 where they fit (else <= 1/2).  out8 receives chunk,
+ * slots_log2, tiny, blocks_per_sm, warps_per_cta, pairs, sparse and a
+ * reserved 0.  Results are identical for every setting. */
 int tchll_set_count_tuning(int32_t chunk, int32_t slots_log2, int32_t tiny, int32_t blocks_per_sm);
 int tchll_set_count_shape(int32_t warps_per_cta, int32_t pairs);
-int tchll_get_count_tuning(int32_t* out6 /* host */);
+int tchll_set_count_table(int32_t sparse);
+int tchll_get_count_tuning(int32_t* out8 /* host */);
 
 /*
  * Allocation-free exact count, for callers that cannot allocate device memory

@@ -45,7 +45,7 @@ def test_host_only_entry_points():
     nb = C.c_size_t(0)
     assert L.tchll_count_workspace_bytes(100, 1000, C.byref(nb)) == 0 and nb.value > 8000
     assert L.tchll_gen_lattice_count(1000, 1000) == 1000 * 999 * 2 + 999 * 999
-    out = (C.c_int32 * 6)()
+    out = (C.c_int32 * 8)()
     assert L.tchll_get_count_tuning(C.cast(out, C.c_void_p)) == 0
     # invalid arguments are rejected on the host with TCHLL_EINVAL
     assert L.tchll_set_count_tuning(33, 11, 16, 0) == _lib.TCHLL_EINVAL

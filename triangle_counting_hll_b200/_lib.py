@@ -66,6 +66,7 @@ SIGNATURES = {
                                              _I32, _P, _P, _P, _P, _P, _P, _SZ, _P]),
     "tchll_set_count_tuning": (C.c_int, [_I32, _I32, _I32, _I32]),
     "tchll_set_count_shape": (C.c_int, [_I32, _I32]),
+    "tchll_set_count_table": (C.c_int, [_I32]),
     "tchll_get_count_tuning": (C.c_int, [_P]),
     "tchll_exact_count_noalloc": (C.c_int, [_P, _I64, _P, _I64, _P, _P, _I64, _P, _P]),
     "tchll_set_phase_timing": (C.c_int, [_I32]),

@@ -240,11 +240,13 @@ def hybrid_count_compact_tensors(row_ptr, col_idx, edge_u, edge_v, degrees, rows
     return res, pe
 
 
-def set_count_tuning(chunk: int = 64, slots_log2: int = 11, tiny: int = 16, blocks_per_sm: int = 0,
-                     warps: Optional[int] = None, pairs: Optional[bool] = None) -> None:
+def set_count_tuning(chunk: int = 256, slots_log2: int = 11, tiny: int = 16, blocks_per_sm: int = 0,
+                     warps: Optional[int] = None, pairs: Optional[bool] = None,
+                     sparse: Optional[bool] = None) -> None:
     """Launch shape of the counting kernels (results do not depend on it)."""
     L = load()
     cur = get_count_tuning()
+    check(L.tchll_set_count_table(int(cur["sparse"] if sparse is None else bool(sparse))))
     w = cur["warps"] if warps is None else int(warps)
     pr = cur["pairs"] if pairs is None else int(bool(pairs))
     # one warp fits every table size, so go through it to reach any valid shape
@@ -254,10 +256,10 @@ def set_count_tuning(chunk: int = 64, slots_log2: int = 11, tiny: int = 16, bloc
 
 
 def get_count_tuning() -> dict:
-    out = (C.c_int32 * 6)()
+    out = (C.c_int32 * 8)()
     check(load().tchll_get_count_tuning(C.cast(out, C.c_void_p)))
     return {"chunk": out[0], "slots_log2": out[1], "tiny": out[2], "blocks_per_sm": out[3], "warps": out[4],
-            "pairs": out[5]}
+            "pairs": out[5], "sparse": out[6]}
 
 
 def set_phase_timing(enable: bool) -> None:

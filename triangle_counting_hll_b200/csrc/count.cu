@@ -78,6 +78,7 @@ struct CountParams {
     int chunk;
     int slots_log2;  // per-warp table capacity (log2 slots)
     int tiny;        // lane-local merge when |N+x| + |N+y| <= tiny
+    int sparse;      // 1: table load <= 1/4 where it fits (else <= 1/2)
 };
 
 // Bucketized cuckoo table: 2^lgb buckets of two int32 slots (one 8-byte
@@ -104,9 +105,9 @@ __device__ __forceinline__ uint32_t tbl_lookup(const int2* T, int32_t x, int lgb
     return (uint32_t)((p.x == x) | (p.y == x) | (q.x == x) | (q.y == x));
 }
 
-// Inserts x (lane-parallel, shared-memory atomics).  Returns false when the
-// key could not be placed within the kick budget (the caller then falls back
-// to binary search for this table side).
+// Inserts x (lane-parallel, shared-memory atomics; empty slots hold -1).
+// Returns false when the key could not be placed within the kick budget (the
+// caller then falls back to binary search for this table side).
 __device__ __forceinline__ bool tbl_insert(int32_t* T, int32_t x, int lgb) {
     const Buckets xb = tbl_buckets(x, lgb);
     if (atomicCAS(T + 2 * xb.b1, -1, x) == -1) return true;
@@ -337,12 +338,14 @@ __global__ void __launch_bounds__(256, 1) count_kernel(const CountParams P) {
                 }
                 if (ucur != cur_u) {
                     // (re)build the warp's table for N+(ucur): 2^lgb buckets,
-                    // load gdu / 2^(lgb+1) <= 1/2
-                    int lgb = ceil_log2_i(gdu);
-                    lgb = lgb < 4 ? 4 : lgb;
+                    // load gdu / 2^(lgb+1) <= 1/4 when the capacity allows,
+                    // <= 1/2 always
+                    int lgb = ceil_log2_i(gdu) + (P.sparse ? 1 : 0);
+                    lgb = lgb < 4 ? 4 : (lgb > cap_lg - 1 ? cap_lg - 1 : lgb);
                     const int nslots = 2 << lgb;
                     __syncwarp();
-                    for (int i = lane; i < nslots; i += 32) table[i] = -1;
+                    for (int i = lane; i < (nslots >> 2); i += 32)
+                        reinterpret_cast<int4*>(table)[i] = make_int4(-1, -1, -1, -1);
                     __syncwarp();
                     bool ok = true;
                     for (int i = lane; i < gdu; i += 32) ok &= tbl_insert(table, __ldg(col_idx + gus + i), lgb);
@@ -524,12 +527,13 @@ __global__ void __launch_bounds__(256, 1) count_kernel(const CountParams P) {
 
 // ---------------------------------------------------------------- host ------
 struct Tuning {
-    int chunk = 64;
+    int chunk = 256;
     int slots_log2 = 11;    // 2048 slots = 8 KB per warp
     int tiny = 16;
     int blocks_per_sm = 0;  // 0: occupancy maximum
     int warps = 8;          // warps per CTA
     int pairs = 1;          // table-side / probe-side reorientation
+    int sparse = 0;         // table load <= 1/4 where it fits
 };
 static Tuning g_tuning;
 
@@ -651,6 +655,7 @@ static int run_count(CountParams P, int mode, bool details, void* ws, size_t ws_
     P.chunk = g_tuning.chunk;
     P.slots_log2 = g_tuning.slots_log2;
     P.tiny = g_tuning.tiny;
+    P.sparse = g_tuning.sparse;
     P.n_edges_dev = nullptr;
     if (P.n_edges == 0) return TCHLL_OK;
     const bool pairs = g_tuning.pairs && !details;
@@ -843,14 +848,21 @@ TCHLL_EXPORT int tchll_set_count_shape(int32_t warps_per_cta, int32_t pairs) {
     return TCHLL_OK;
 }
 
-TCHLL_EXPORT int tchll_get_count_tuning(int32_t* out6) {
-    TCHLL_ARG(out6 != nullptr, "out is null");
-    out6[0] = g_tuning.chunk;
-    out6[1] = g_tuning.slots_log2;
-    out6[2] = g_tuning.tiny;
-    out6[3] = g_tuning.blocks_per_sm;
-    out6[4] = g_tuning.warps;
-    out6[5] = g_tuning.pairs;
+TCHLL_EXPORT int tchll_set_count_table(int32_t sparse) {
+    g_tuning.sparse = sparse ? 1 : 0;
+    return TCHLL_OK;
+}
+
+TCHLL_EXPORT int tchll_get_count_tuning(int32_t* out8) {
+    TCHLL_ARG(out8 != nullptr, "out is null");
+    out8[0] = g_tuning.chunk;
+    out8[1] = g_tuning.slots_log2;
+    out8[2] = g_tuning.tiny;
+    out8[3] = g_tuning.blocks_per_sm;
+    out8[4] = g_tuning.warps;
+    out8[5] = g_tuning.pairs;
+    out8[6] = g_tuning.sparse;
+    out8[7] = 0;  // reserved
     return TCHLL_OK;
 }
 
