@@ -205,6 +205,45 @@ int tchll_hll_estimate_pairs(const uint8_t* rows, int64_t n_rows, int32_t p, con
 /* _hash64 (src/hll.py:13-19) of n int64 values. */
 int tchll_hash64(const int64_t* values, int64_t n, uint64_t* out, void* stream);
 
+/* ------------------------------------------------------------ batched --- */
+/*
+ * Many graphs in one launch (no counterpart in the reference, which counts
+ * one graph per call).  The graphs share one CSR with disjoint vertex ranges
+ * [graph_vbase[g], graph_vbase[g+1]) -- offset each graph's ids before
+ * tchll_csr_build_phase1 and take the ranges from the compacted node table --
+ * and edge_u/edge_v must be the CSR's own edge list (graph g's edges are
+ * positions [row_ptr[vbase[g]], row_ptr[vbase[g+1]])).  results[n_graphs]
+ * receives one tchll_count_result per graph, bit-identical to counting that
+ * graph alone (an edge outside its graph's range sets status on that graph).
+ * Work is a device-built list of chunks that never cross a graph, claimed by
+ * one persistent launch.
+ */
+int tchll_batch_workspace_bytes(int64_t n_nodes, int64_t n_edges, int64_t n_graphs, size_t* bytes);
+int tchll_batch_exact_count(const int32_t* row_ptr, int64_t n_nodes, const int32_t* col_idx, int64_t nnz,
+                            const int32_t* edge_u, const int32_t* edge_v, int64_t n_edges,
+                            const int32_t* graph_vbase, int64_t n_graphs, tchll_count_result* results,
+                            void* workspace, size_t workspace_bytes, void* stream);
+/* Hybrid per graph (split exact / HLL launches, compact sketches). */
+int tchll_batch_hybrid_count(const int32_t* row_ptr, int64_t n_nodes, const int32_t* col_idx, int64_t nnz,
+                             const int32_t* edge_u, const int32_t* edge_v, int64_t n_edges, const int32_t* degrees,
+                             const uint8_t* rows, int64_t n_rows, const int64_t* slot, int32_t p, int64_t gamma,
+                             const int32_t* graph_vbase, int64_t n_graphs, tchll_count_result* results,
+                             void* workspace, size_t workspace_bytes, void* stream);
+/* local_ids[v] = v - graph_vbase[g] for v in graph g (v outside every range
+ * keeps v): the key table for tchll_build_sketches_compact that makes batched
+ * sketches hash the same ids as each graph's own CSR. */
+int tchll_batch_local_ids(const int32_t* graph_vbase, int64_t n_graphs, int64_t n_nodes, int64_t* local_ids,
+                          void* stream);
+
+/*
+ * Degree statistics (experiment/gpu_graph_stats.py:100-140): over vertices of
+ * positive degree (degrees[v], or row_ptr[v+1]-row_ptr[v] when degrees is
+ * NULL), sums3 = {count, sum d, sum d^2}, minmax2 = {max, min}, and
+ * log_hist32[b] = number with floor(log2 d) == b (b capped at 31).
+ */
+int tchll_degree_stats(const int32_t* degrees, const int32_t* row_ptr, int64_t n, uint64_t* log_hist32,
+                       uint64_t* sums3, int32_t* minmax2, void* stream);
+
 /* -------------------------------------------------- CSR construction --- */
 /*
  * Edge list -> oriented CSR, the array form of orient_graph + to_csr_numpy

@@ -1,0 +1,135 @@
+"""Batched counting (many graphs in one launch) and the degree-keyed autotuner.
+
+GPU tests check that per-graph results of the batched launch are bit-identical
+to counting each graph alone (exact counts, hybrid fixed-point totals and
+stats) and to the oracle; CPU tests cover the host-side workload generator
+and the autotuner's signature.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+
+def test_c4_specs_distribution():
+    from triangle_counting_hll_b200.batch import c4_specs
+    specs = c4_specs(2048)
+    ns = np.array([s.n for s in specs])
+    assert len(specs) == 2048 and ns.min() >= 500 and ns.max() <= 500000
+    assert 4000 < np.median(ns) < 6000
+    assert [s.kind for s in specs[:4]] == ["er", "chung_lu", "er", "chung_lu"]
+    assert [s.seed for s in specs[:3]] == [0, 1, 2]
+    assert c4_specs(16) == c4_specs(16)  # deterministic
+
+
+def test_autotune_signature_is_shape_key():
+    from triangle_counting_hll_b200.autotune import signature
+    h = np.zeros(32, dtype=np.int64)
+    h[:4] = [100, 50, 20, 5]
+    s1 = signature({"log_hist": h})
+    s2 = signature({"log_hist": h * 10})  # same shape, 10x the vertices
+    assert s1 == s2 and s1.startswith("top3:")
+    h2 = h.copy()
+    h2[10] = 3
+    assert signature({"log_hist": h2}) != s1
+    assert signature({"log_hist": np.zeros(32)}) == "empty"
+
+
+def _small_batch(dev, n_graphs=40):
+    import torch
+    from triangle_counting_hll_b200 import batch as B
+    specs = B.c4_specs(n_graphs, median=800, sigma=0.8, lo=50, hi=5000, seed_base=11)
+    graphs = [B.generate(s, dev) for s in specs]
+    items = [(u, v, s.n) for (u, v), s in zip(graphs, specs)]
+    # edge cases: an empty graph, a single edge, a triangle, a dense clique
+    z = torch.zeros(0, dtype=torch.int32, device=dev)
+    items.insert(3, (z, z, 10))
+    items.insert(7, (torch.tensor([4], dtype=torch.int32, device=dev), torch.tensor([2], dtype=torch.int32,
+                                                                                    device=dev), 5))
+    items.append((torch.tensor([0, 1, 2], dtype=torch.int32, device=dev),
+                  torch.tensor([1, 2, 0], dtype=torch.int32, device=dev), 3))
+    iu, iv = np.triu_indices(60, 1)
+    items.append((torch.from_numpy(iu.astype(np.int32)).to(dev), torch.from_numpy(iv.astype(np.int32)).to(dev), 60))
+    return items
+
+
+@pytest.mark.gpu
+def test_batched_exact_bit_exact_vs_one_at_a_time(tchll, oracle):
+    import torch
+    from triangle_counting_hll_b200 import batch as B
+    from triangle_counting_hll_b200 import core
+    dev = torch.device("cuda", 0)
+    items = _small_batch(dev)
+    bt = B.GraphBatch.from_edge_lists(items, device=dev)
+    got = bt.exact_counts()
+    csrs = [core.csr_from_edges(u, v, device=dev) for u, v, _ in items]
+    ref = B.plain_exact_counts(csrs)
+    assert np.array_equal(got, ref)
+    # and against the oracle, graph by graph
+    for (u, v, _), c in zip(items, got):
+        og = oracle.csr_build(u.cpu().numpy(), v.cpu().numpy())
+        assert c == oracle.exact_count(og["row_ptr"], og["col_idx"], og["edge_u"], og["edge_v"])
+    assert got[-1] == 60 * 59 * 58 // 6 and got[-2] == 1 and got[3] == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("theta,p", [(8, 10), (16, 8), (4, 12)])
+def test_batched_hybrid_bit_exact_vs_one_at_a_time(tchll, theta, p):
+    import torch
+    from triangle_counting_hll_b200 import batch as B
+    from triangle_counting_hll_b200 import core
+    dev = torch.device("cuda", 0)
+    items = _small_batch(dev)
+    bt = B.GraphBatch.from_edge_lists(items, device=dev)
+    tot, st = bt.hybrid_counts(theta, theta, p)
+    csrs = [core.csr_from_edges(u, v, device=dev) for u, v, _ in items]
+    rtot, rst = B.plain_hybrid_counts(csrs, B.plain_sketches(csrs, theta, p), theta, p)
+    assert np.array_equal(tot, rtot)  # fixed-point sums: bit-identical
+    for k in rst:
+        assert np.array_equal(st[k], rst[k]), k
+    assert st["n_approx"].sum() > 0  # the HLL path ran
+    ex = bt.exact_counts()
+    assert np.array_equal(st["n_approx"] + st["n_exact"], np.array([c.n_edges for c in csrs]))
+    assert (tot[st["n_approx"] == 0] == ex[st["n_approx"] == 0]).all()
+
+
+@pytest.mark.gpu
+def test_captured_batch_replays_and_tuning(tchll):
+    import torch
+    from triangle_counting_hll_b200 import autotune, batch as B, core
+    dev = torch.device("cuda", 0)
+    items = _small_batch(dev, 24)
+    bt = B.GraphBatch.from_edge_lists(items, device=dev)
+    ref = bt.exact_counts()
+    base = core.get_count_tuning()
+    try:
+        cfg = autotune.tune_batch(bt, autotune.Autotuner())
+        assert cfg["key"].startswith("top")
+        cap = B.CapturedBatch(bt)
+        a = cap.exact_counts()
+        b = cap.exact_counts()
+        assert np.array_equal(a, ref) and np.array_equal(b, ref)
+        caph = B.CapturedBatch(bt, hybrid=(8, 8, 10))
+        t1, s1 = caph.hybrid_counts()
+        t2, s2 = caph.hybrid_counts()
+        t3, s3 = bt.hybrid_counts(8, 8, 10)
+        assert np.array_equal(t1, t2) and np.array_equal(t1, t3)
+    finally:
+        core.set_count_tuning(**{k: base[k] for k in ("chunk", "slots_log2", "tiny", "blocks_per_sm", "warps",
+                                                       "pairs", "sparse")})
+
+
+@pytest.mark.gpu
+def test_degree_stats_match_numpy(tchll):
+    import torch
+    from triangle_counting_hll_b200 import autotune, core
+    dev = torch.device("cuda", 0)
+    u, v = core.gen_rmat(14, 16, 0.57, 0.19, 0.19, seed=3, device=dev)
+    g = core.csr_from_edges(u, v)
+    st = autotune.degree_stats(g.row_ptr)
+    d = np.diff(g.row_ptr.cpu().numpy().astype(np.int64))
+    dp = d[d > 0]
+    assert st["active"] == len(dp) and st["sum"] == dp.sum() and st["sumsq"] == (dp * dp).sum()
+    assert st["max"] == dp.max() and st["min"] == dp.min()
+    ref = np.bincount(np.floor(np.log2(dp)).astype(int), minlength=32)[:32]
+    assert np.array_equal(st["log_hist"], ref)

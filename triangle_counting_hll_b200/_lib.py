@@ -84,6 +84,12 @@ SIGNATURES = {
     "tchll_adj_workspace_bytes": (C.c_int, [_I64, _I64, C.POINTER(_SZ)]),
     "tchll_csr_from_adjacency": (C.c_int, [_P, _P, _I64, _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _P, _SZ,
                                            _P]),
+    "tchll_batch_workspace_bytes": (C.c_int, [_I64, _I64, _I64, C.POINTER(_SZ)]),
+    "tchll_batch_exact_count": (C.c_int, [_P, _I64, _P, _I64, _P, _P, _I64, _P, _I64, _P, _P, _SZ, _P]),
+    "tchll_batch_hybrid_count": (C.c_int, [_P, _I64, _P, _I64, _P, _P, _I64, _P, _P, _I64, _P, _I32, _I64, _P, _I64,
+                                           _P, _P, _SZ, _P]),
+    "tchll_batch_local_ids": (C.c_int, [_P, _I64, _I64, _P, _P]),
+    "tchll_degree_stats": (C.c_int, [_P, _P, _I64, _P, _P, _P, _P]),
     "tchll_ingest_workspace_bytes": (C.c_int, [_I64, C.POINTER(_SZ)]),
     "tchll_parse_edges": (C.c_int, [_P, _I64, C.c_char_p, _P, _P, _P, _P, _P, _SZ, _P]),
     "tchll_gen_rmat": (C.c_int, [_I32, _I64, _U32, _U32, _U32, _U64, _P, _P, _P]),

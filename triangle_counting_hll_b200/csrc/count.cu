@@ -79,6 +79,14 @@ struct CountParams {
     int slots_log2;  // per-warp table capacity (log2 slots)
     int tiny;        // lane-local merge when |N+x| + |N+y| <= tiny
     int sparse;      // 1: table load <= 1/4 where it fits (else <= 1/2)
+    // Batched mode: work units are chunks [chunk_start[i], +chunk_len[i]) of
+    // one graph each (never crossing a graph), claimed one at a time; each
+    // chunk's totals go to results[chunk_graph[i]].
+    const int64_t* chunk_start;
+    const int32_t* chunk_len;
+    const int32_t* chunk_graph;
+    const int64_t* n_chunks_dev;
+    const int32_t* graph_vbase;  // vertex range of graph g: [vbase[g], vbase[g+1])
 };
 
 // Bucketized cuckoo table: 2^lgb buckets of two int32 slots (one 8-byte
@@ -256,6 +264,28 @@ __device__ __forceinline__ uint32_t lane_merge_count(const int32_t* a, int la, c
     return c;
 }
 
+// Warp-reduces the per-lane totals and adds them to *R (lane 0, integer
+// atomics; order-independent).
+__device__ __forceinline__ void publish(tchll_count_result* R, uint64_t acc, U128 hacc, int64_t n_approx,
+                                        int64_t n_exact, int64_t n_fallback, int64_t n_clamped, uint32_t status,
+                                        int lane) {
+    acc = warp_sum_u64(acc);
+    n_approx = warp_sum_i64(n_approx);
+    n_exact = warp_sum_i64(n_exact);
+    n_fallback = warp_sum_i64(n_fallback);
+    n_clamped = warp_sum_i64(n_clamped);
+    status = __reduce_or_sync(FULL, status);
+    if (lane == 0) {
+        if (acc) atomicAdd((unsigned long long*)&R->exact, (unsigned long long)acc);
+        atomic_add_u128((unsigned long long*)&R->hll_fx_lo, hacc);
+        if (n_approx) atomicAdd((unsigned long long*)&R->n_approx, (unsigned long long)n_approx);
+        if (n_exact) atomicAdd((unsigned long long*)&R->n_exact, (unsigned long long)n_exact);
+        if (n_fallback) atomicAdd((unsigned long long*)&R->n_fallback, (unsigned long long)n_fallback);
+        if (n_clamped) atomicAdd((unsigned long long*)&R->n_clamped, (unsigned long long)n_clamped);
+        if (status) atomicOr(&R->status, status);
+    }
+}
+
 template <int MODE, bool VEC, bool DETAILS>
 __global__ void __launch_bounds__(256, 1) count_kernel(const CountParams P) {
     extern __shared__ __align__(16) int32_t smem[];
@@ -278,14 +308,34 @@ __global__ void __launch_bounds__(256, 1) count_kernel(const CountParams P) {
 
     while (true) {
         unsigned long long e0 = 0;
-        if (lane == 0) e0 = atomicAdd(P.work, (unsigned long long)P.chunk);
-        e0 = __shfl_sync(FULL, e0, 0);
-        if (e0 >= (unsigned long long)n_edges) break;
-        const int64_t e1 = min((int64_t)e0 + P.chunk, n_edges);
+        int64_t e1;
+        int32_t gcur = -1;
+        if (P.chunk_start) {
+            unsigned long long ci = 0;
+            if (lane == 0) ci = atomicAdd(P.work, 1ull);
+            ci = __shfl_sync(FULL, ci, 0);
+            if ((int64_t)ci >= *P.n_chunks_dev) break;
+            e0 = (unsigned long long)__ldg(P.chunk_start + ci);
+            e1 = (int64_t)e0 + __ldg(P.chunk_len + ci);
+            gcur = __ldg(P.chunk_graph + ci);
+        } else {
+            if (lane == 0) e0 = atomicAdd(P.work, (unsigned long long)P.chunk);
+            e0 = __shfl_sync(FULL, e0, 0);
+            if (e0 >= (unsigned long long)n_edges) break;
+            e1 = min((int64_t)e0 + P.chunk, n_edges);
+        }
         for (int64_t eb = (int64_t)e0; eb < e1; eb += 32) {
             const int64_t e = eb + lane;
             int32_t u = 0, v = 0, us = 0, ue = 0, vs = 0, ve = 0;
             bool valid = e < e1 && load_edge(P, e, u, v, us, ue, vs, ve, status);
+            if (valid && gcur >= 0) {
+                // an edge of another graph inside this graph's chunk
+                const int32_t lo_v = __ldg(P.graph_vbase + gcur), hi_v = __ldg(P.graph_vbase + gcur + 1);
+                if (u < lo_v || u >= hi_v || v < lo_v || v >= hi_v) {
+                    status |= ST_BAD_EDGE;
+                    valid = false;
+                }
+            }
             bool is_hll = false;
             int64_t slot_u = -1, slot_v = -1;
             int32_t du = 0, dv = 0;
@@ -504,25 +554,17 @@ __global__ void __launch_bounds__(256, 1) count_kernel(const CountParams P) {
                 }
             }
         }
+        if (gcur >= 0) {  // batched: this chunk's totals belong to graph gcur
+            publish(P.result + gcur, acc, hacc, n_approx, n_exact, n_fallback, n_clamped, status, lane);
+            acc = 0;
+            hacc = U128();
+            n_approx = n_exact = n_fallback = n_clamped = 0;
+            status = 0;
+        }
     }
 
     // ---------------------------------------------------------- publish ----
-    acc = warp_sum_u64(acc);
-    n_approx = warp_sum_i64(n_approx);
-    n_exact = warp_sum_i64(n_exact);
-    n_fallback = warp_sum_i64(n_fallback);
-    n_clamped = warp_sum_i64(n_clamped);
-    status = __reduce_or_sync(FULL, status);
-    if (lane == 0) {
-        tchll_count_result* R = P.result;
-        if (acc) atomicAdd((unsigned long long*)&R->exact, (unsigned long long)acc);
-        atomic_add_u128((unsigned long long*)&R->hll_fx_lo, hacc);
-        if (n_approx) atomicAdd((unsigned long long*)&R->n_approx, (unsigned long long)n_approx);
-        if (n_exact) atomicAdd((unsigned long long*)&R->n_exact, (unsigned long long)n_exact);
-        if (n_fallback) atomicAdd((unsigned long long*)&R->n_fallback, (unsigned long long)n_fallback);
-        if (n_clamped) atomicAdd((unsigned long long*)&R->n_clamped, (unsigned long long)n_clamped);
-        if (status) atomicOr(&R->status, status);
-    }
+    if (!P.chunk_start) publish(P.result, acc, hacc, n_approx, n_exact, n_fallback, n_clamped, status, lane);
 }
 
 // ---------------------------------------------------------------- host ------
@@ -619,26 +661,39 @@ static int grid_edges(int64_t n) {
     return g < 1 ? 1 : (int)g;
 }
 
-// Build the grouped (x, y) pair list of the exact edges into Q.
+// Pair regrouping, part 1: histogram of table sides and its exclusive scan
+// (W.off[x] = first pair of x, W.off[n_nodes] = number of pairs).
 template <bool HYB>
-static int build_pairs(const CountParams& P, const CountWs& W, CountParams& Q, cudaStream_t st) {
+static int pairs_hist_scan(const CountParams& P, const CountWs& W, cudaStream_t st) {
     const int64_t N = P.n_nodes + 1;
     TCHLL_CUDA(cudaMemsetAsync(W.cnt, 0, sizeof(int32_t) * N, st));
-    const int g = grid_edges(P.n_edges);
-    pair_hist_kernel<HYB><<<g, 256, 0, st>>>(P, W.cnt);
+    pair_hist_kernel<HYB><<<grid_edges(P.n_edges), 256, 0, st>>>(P, W.cnt);
     TCHLL_CHECK_LAUNCH("pair_hist_kernel");
     size_t tb = W.tmp_bytes;
     TCHLL_CUDA(cub::DeviceScan::ExclusiveSum(W.tmp, tb, W.cnt, W.off, (int)N, st));
     count_launch();
-    // W.off[n_nodes] is the number of pairs; the scatter advances off[x] for
-    // x < n_nodes only, so the total survives.
-    pair_scatter_kernel<HYB><<<g, 256, 0, st>>>(P, W.off, W.px, W.py);
+    return TCHLL_OK;
+}
+
+// Part 2: scatter the pairs (advances W.off[x] for x < n_nodes only, so the
+// total in W.off[n_nodes] survives) and point Q at the pair list.
+template <bool HYB>
+static int pairs_scatter(const CountParams& P, const CountWs& W, CountParams& Q, cudaStream_t st) {
+    pair_scatter_kernel<HYB><<<grid_edges(P.n_edges), 256, 0, st>>>(P, W.off, W.px, W.py);
     TCHLL_CHECK_LAUNCH("pair_scatter_kernel");
     Q = P;
     Q.edge_u = W.px;
     Q.edge_v = W.py;
     Q.n_edges_dev = W.off + P.n_nodes;
     return TCHLL_OK;
+}
+
+// Build the grouped (x, y) pair list of the exact edges into Q.
+template <bool HYB>
+static int build_pairs(const CountParams& P, const CountWs& W, CountParams& Q, cudaStream_t st) {
+    int rc = pairs_hist_scan<HYB>(P, W, st);
+    if (rc) return rc;
+    return pairs_scatter<HYB>(P, W, Q, st);
 }
 
 static int run_count(CountParams P, int mode, bool details, void* ws, size_t ws_bytes, cudaStream_t st) {
@@ -953,4 +1008,241 @@ TCHLL_EXPORT int tchll_exact_count_noalloc(const int32_t* row_ptr, int64_t n_nod
     // before any kernel reads them, so leftovers of the previous call are
     // harmless; calls that overlap on the GPU would share the array and race.
     return run_count(P, MODE_EXACT, false, scratch, TCHLL_NOALLOC_SCRATCH_BYTES, (cudaStream_t)stream);
+}
+
+// ------------------------------------------------------------- batched ------
+// Many graphs in one launch.  The graphs share one CSR with disjoint vertex
+// ranges [vbase[g], vbase[g+1]) (ids offset per graph before the CSR build:
+// orientation and compaction are per vertex, so each graph's part of the CSR
+// equals its own CSR shifted).  Work is a list of chunks that never cross a
+// graph; each chunk adds its integer totals to results[g], so per-graph
+// results are bit-identical to one graph at a time.
+
+// A graph whose vertex range is malformed gets no chunks (and a status flag
+// from check_vbase_kernel); no vbase entry is used as an index unchecked.
+__device__ __forceinline__ bool graph_range(const int32_t* base, const int32_t* vbase, int64_t g, int64_t n_nodes,
+                                            int64_t& s0, int64_t& s1) {
+    const int32_t a = vbase[g], b = vbase[g + 1];
+    if (a < 0 || b < a || (int64_t)b > n_nodes) return false;
+    s0 = base[a];
+    s1 = base[b];
+    return s1 >= s0;
+}
+
+__global__ void chunk_count_kernel(const int32_t* __restrict__ base, const int32_t* __restrict__ vbase,
+                                   int64_t n_graphs, int64_t n_nodes, int chunk, int64_t* cnt) {
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g <= n_graphs;
+         g += (int64_t)gridDim.x * blockDim.x) {
+        if (g == n_graphs) {
+            cnt[g] = 0;
+            continue;
+        }
+        int64_t s0, s1;
+        cnt[g] = graph_range(base, vbase, g, n_nodes, s0, s1) ? (s1 - s0 + chunk - 1) / chunk : 0;
+    }
+}
+
+__global__ void chunk_fill_kernel(const int32_t* __restrict__ base, const int32_t* __restrict__ vbase,
+                                  int64_t n_graphs, int64_t n_nodes, int chunk, const int64_t* __restrict__ coff,
+                                  int64_t* cstart, int32_t* clen, int32_t* cgraph) {
+    // one warp per graph
+    const int lane = threadIdx.x & 31;
+    for (int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; g < n_graphs;
+         g += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        int64_t s0 = 0, s1 = 0;
+        if (!graph_range(base, vbase, g, n_nodes, s0, s1)) continue;
+        const int64_t n = coff[g + 1] - coff[g];
+        for (int64_t k = lane; k < n; k += 32) {
+            const int64_t st = s0 + k * chunk;
+            cstart[coff[g] + k] = st;
+            clen[coff[g] + k] = (int32_t)min((int64_t)chunk, s1 - st);
+            cgraph[coff[g] + k] = (int32_t)g;
+        }
+    }
+}
+
+__global__ void check_vbase_kernel(const int32_t* __restrict__ vbase, int64_t n_graphs, int64_t n_nodes,
+                                   tchll_count_result* results) {
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_graphs;
+         g += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t a = vbase[g], b = vbase[g + 1];
+        if (a < 0 || b < a || (int64_t)b > n_nodes) results[g].status |= ST_BAD_ROW;
+    }
+}
+
+struct BatchWs {
+    CountWs cw;
+    int64_t* cnt;     // n_graphs + 1
+    int64_t* coff;    // n_graphs + 1 (last entry: number of chunks)
+    int64_t* cstart;  // max chunks
+    int32_t* clen;
+    int32_t* cgraph;
+    void* tmp;
+    size_t tmp_bytes;
+};
+
+static int64_t max_chunks(int64_t n_edges, int64_t n_graphs, int chunk) {
+    return n_edges / chunk + n_graphs + 1;
+}
+
+static bool carve_batch(void* ws, size_t bytes, int64_t n_nodes, int64_t n_edges, int64_t n_graphs, BatchWs& B,
+                        size_t* need) {
+    size_t cneed = 0;
+    carve_count(nullptr, 0, n_nodes, n_edges, B.cw, &cneed);
+    const size_t G = (size_t)n_graphs + 1;
+    const size_t MC = (size_t)max_chunks(n_edges, n_graphs, 32);  // any chunk size >= 32 fits
+    size_t tb = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tb, (int64_t*)nullptr, (int64_t*)nullptr, (int)G);
+    Carve cv(ws, bytes);
+    char* cbase = cv.take<char>(cneed);
+    B.cnt = cv.take<int64_t>(G);
+    B.coff = cv.take<int64_t>(G);
+    B.cstart = cv.take<int64_t>(MC);
+    B.clen = cv.take<int32_t>(MC);
+    B.cgraph = cv.take<int32_t>(MC);
+    B.tmp_bytes = tb;
+    B.tmp = cv.take<char>(tb);
+    if (need) *need = cv.off;
+    if (!cv.ok() || cv.dry) return cv.ok();
+    carve_count(cbase, cneed, n_nodes, n_edges, B.cw, nullptr);
+    return true;
+}
+
+// Chunk list over per-graph ranges [base[vbase[g]], base[vbase[g+1]]).
+static int build_chunks(const int32_t* base, const int32_t* vbase, int64_t n_graphs, int64_t n_nodes,
+                        const BatchWs& B, cudaStream_t st) {
+    const int chunk = g_tuning.chunk;
+    int64_t g = (n_graphs + 256) / 256;
+    if (g > (int64_t)sm_count() * 8) g = (int64_t)sm_count() * 8;
+    chunk_count_kernel<<<(int)g, 256, 0, st>>>(base, vbase, n_graphs, n_nodes, chunk, B.cnt);
+    TCHLL_CHECK_LAUNCH("chunk_count_kernel");
+    size_t tb = B.tmp_bytes;
+    TCHLL_CUDA(cub::DeviceScan::ExclusiveSum(B.tmp, tb, B.cnt, B.coff, (int)(n_graphs + 1), st));
+    count_launch();
+    int64_t gw = (n_graphs * 32 + 255) / 256;
+    if (gw > (int64_t)sm_count() * 8) gw = (int64_t)sm_count() * 8;
+    if (gw < 1) gw = 1;
+    chunk_fill_kernel<<<(int)gw, 256, 0, st>>>(base, vbase, n_graphs, n_nodes, chunk, B.coff, B.cstart, B.clen,
+                                               B.cgraph);
+    TCHLL_CHECK_LAUNCH("chunk_fill_kernel");
+    return TCHLL_OK;
+}
+
+static int run_batch(CountParams P, bool hybrid, const int32_t* vbase, int64_t n_graphs, void* ws, size_t wsb,
+                     cudaStream_t st) {
+    BatchWs B;
+    size_t need = 0;
+    if (!carve_batch(ws, wsb, P.n_nodes, P.n_edges, n_graphs, B, &need) || ws == nullptr) {
+        set_error("workspace too small: need %zu bytes, have %zu", need, wsb);
+        return TCHLL_EWORKSPACE;
+    }
+    TCHLL_CUDA(cudaMemsetAsync(P.result, 0, sizeof(tchll_count_result) * n_graphs, st));
+    TCHLL_CUDA(cudaMemsetAsync(B.cw.ctr, 0, 4 * sizeof(unsigned long long), st));
+    if (n_graphs == 0) return TCHLL_OK;
+    {
+        int64_t g = (n_graphs + 255) / 256;
+        if (g > 1024) g = 1024;
+        check_vbase_kernel<<<(int)g, 256, 0, st>>>(vbase, n_graphs, P.n_nodes, P.result);
+        TCHLL_CHECK_LAUNCH("check_vbase_kernel");
+    }
+    P.chunk = g_tuning.chunk;
+    P.slots_log2 = g_tuning.slots_log2;
+    P.tiny = g_tuning.tiny;
+    P.sparse = g_tuning.sparse;
+    P.n_edges_dev = nullptr;
+    P.graph_vbase = vbase;
+    P.n_chunks_dev = B.coff + n_graphs;
+    P.chunk_start = B.cstart;
+    P.chunk_len = B.clen;
+    P.chunk_graph = B.cgraph;
+    if (P.n_edges == 0) return TCHLL_OK;
+    int rc;
+    CountParams Q;
+    phase_reset();
+    P.work = B.cw.ctr;
+    phase_mark(0, st);
+    if (hybrid) rc = pairs_hist_scan<true>(P, B.cw, st);
+    else rc = pairs_hist_scan<false>(P, B.cw, st);
+    if (rc) return rc;
+    rc = build_chunks(B.cw.off, vbase, n_graphs, P.n_nodes, B, st);  // pair ranges (before the scatter)
+    if (rc) return rc;
+    if (hybrid) rc = pairs_scatter<true>(P, B.cw, Q, st);
+    else rc = pairs_scatter<false>(P, B.cw, Q, st);
+    if (rc) return rc;
+    phase_mark(1, st);
+    Q.n_edges_dev = nullptr;
+    rc = launch_count<MODE_EXACT>(Q, false, st);
+    if (rc) return rc;
+    phase_mark(2, st);
+    g_phase.used[0] = g_phase.used[1] = true;
+    if (!hybrid) return TCHLL_OK;
+    // HLL-routed edges: chunks over each graph's CSR edge range
+    TCHLL_CUDA(cudaMemsetAsync(B.cw.ctr + 1, 0, sizeof(unsigned long long), st));
+    rc = build_chunks(P.row_ptr, vbase, n_graphs, P.n_nodes, B, st);
+    if (rc) return rc;
+    P.work = B.cw.ctr + 1;
+    rc = launch_count<MODE_HYB_HLL>(P, false, st);
+    phase_mark(3, st);
+    g_phase.used[2] = true;
+    return rc;
+}
+
+TCHLL_EXPORT int tchll_batch_workspace_bytes(int64_t n_nodes, int64_t n_edges, int64_t n_graphs, size_t* bytes) {
+    TCHLL_ARG(bytes && n_nodes >= 0 && n_edges >= 0 && n_graphs >= 0, "bad arguments");
+    BatchWs B;
+    carve_batch(nullptr, 0, n_nodes, n_edges, n_graphs, B, bytes);
+    return TCHLL_OK;
+}
+
+TCHLL_EXPORT int tchll_batch_exact_count(const int32_t* row_ptr, int64_t n_nodes, const int32_t* col_idx, int64_t nnz,
+                                         const int32_t* edge_u, const int32_t* edge_v, int64_t n_edges,
+                                         const int32_t* graph_vbase, int64_t n_graphs, tchll_count_result* results,
+                                         void* workspace, size_t workspace_bytes, void* stream) {
+    int rc = check_common(row_ptr, n_nodes, col_idx, nnz, edge_u, edge_v, n_edges, results);
+    if (rc) return rc;
+    TCHLL_ARG(n_graphs >= 0 && (n_graphs == 0 || graph_vbase), "bad graph table");
+    TCHLL_ARG(n_graphs < (int64_t)INT32_MAX, "too many graphs");
+    CountParams P{};
+    P.row_ptr = row_ptr;
+    P.n_nodes = n_nodes;
+    P.col_idx = col_idx;
+    P.nnz = nnz;
+    P.edge_u = edge_u;
+    P.edge_v = edge_v;
+    P.n_edges = n_edges;
+    P.result = results;
+    P.p = 4;
+    return run_batch(P, false, graph_vbase, n_graphs, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+TCHLL_EXPORT int tchll_batch_hybrid_count(const int32_t* row_ptr, int64_t n_nodes, const int32_t* col_idx,
+                                          int64_t nnz, const int32_t* edge_u, const int32_t* edge_v,
+                                          int64_t n_edges, const int32_t* degrees, const uint8_t* rows,
+                                          int64_t n_rows, const int64_t* slot, int32_t p, int64_t gamma,
+                                          const int32_t* graph_vbase, int64_t n_graphs,
+                                          tchll_count_result* results, void* workspace, size_t workspace_bytes,
+                                          void* stream) {
+    int rc = check_common(row_ptr, n_nodes, col_idx, nnz, edge_u, edge_v, n_edges, results);
+    if (rc) return rc;
+    TCHLL_ARG(p >= 4 && p <= 16, "p must be in [4, 16], got %d", p);
+    TCHLL_ARG(n_edges == 0 || (degrees && slot), "degrees / slot are null");
+    TCHLL_ARG(n_rows == 0 || rows, "register rows are null");
+    TCHLL_ARG(n_graphs >= 0 && (n_graphs == 0 || graph_vbase), "bad graph table");
+    TCHLL_ARG(n_graphs < (int64_t)INT32_MAX, "too many graphs");
+    CountParams P{};
+    P.row_ptr = row_ptr;
+    P.n_nodes = n_nodes;
+    P.col_idx = col_idx;
+    P.nnz = nnz;
+    P.edge_u = edge_u;
+    P.edge_v = edge_v;
+    P.n_edges = n_edges;
+    P.degrees = degrees;
+    P.regs = rows;
+    P.n_rows = n_rows;
+    P.slot = slot;
+    P.p = p;
+    P.gamma = gamma;
+    P.result = results;
+    return run_batch(P, true, graph_vbase, n_graphs, workspace, workspace_bytes, (cudaStream_t)stream);
 }
