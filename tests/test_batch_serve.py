@@ -133,3 +133,58 @@ def test_degree_stats_match_numpy(tchll):
     assert st["max"] == dp.max() and st["min"] == dp.min()
     ref = np.bincount(np.floor(np.log2(dp)).astype(int), minlength=32)[:32]
     assert np.array_equal(st["log_hist"], ref)
+
+
+# ------------------------------------------------------------------ serving
+def test_c5_requests_shape():
+    from triangle_counting_hll_b200.serve import c5_requests, estimate_bytes
+    reqs = c5_requests(2000, 100.0, seed=1, repeat_frac=0.2)
+    arr = np.array([r.arrival for r in reqs])
+    assert (np.diff(arr) >= 0).all() and 15 < arr[-1] < 25  # ~2000 / 100 s
+    sc = np.array([r.scale for r in reqs])
+    ef = np.array([r.edge_factor for r in reqs])
+    assert sc.min() >= 12 and sc.max() <= 20 and ef.min() >= 8 and ef.max() <= 32
+    frac = np.mean([r.mode == "hybrid" for r in reqs])
+    assert 0.45 < frac < 0.55
+    keys = [r.key for r in reqs]
+    assert len(set(keys)) < len(keys)  # repeats present
+    assert estimate_bytes(reqs[0]) > 40 * reqs[0].raw_edges()
+
+
+def _serve_mix(dev, n=60, rate=400.0, budget=120e9, scale_range=(8, 12), repeat=0.3):
+    from triangle_counting_hll_b200 import serve as S
+    reqs = S.c5_requests(n, rate, seed=5, scale_range=scale_range, ef_range=(4, 16), repeat_frac=repeat,
+                         p=10, theta=16)
+    srv = S.Server(dev, budget_bytes=budget, max_batch=32)
+    return reqs, srv, srv.serve(reqs)
+
+
+@pytest.mark.gpu
+def test_server_results_same_alone_and_in_the_mix(tchll):
+    import torch
+    from triangle_counting_hll_b200 import serve as S
+    dev = torch.device("cuda", 0)
+    reqs, srv, got = _serve_mix(dev)
+    assert len(got) == len(reqs) and all(c.error is None for c in got)
+    assert srv.stats["ticks"] < len(reqs)          # queries were batched
+    assert max(srv.stats["batch_sizes"]) > 1
+    assert srv.stats["cache_hits"] > 0             # repeat queries reused resident graphs
+    for r, c in zip(sorted(reqs, key=lambda r: r.rid), got):
+        alone = S.answer_alone(r, dev)
+        assert c.value == alone.value and c.stats == alone.stats, r  # bit-identical, exact and hybrid
+
+
+@pytest.mark.gpu
+def test_server_admission_budget_and_rejection(tchll):
+    import torch
+    from triangle_counting_hll_b200 import serve as S
+    dev = torch.device("cuda", 0)
+    small = S.Request(0, 0.0, 8, 4, 1, "exact")
+    huge = S.Request(1, 0.0, 20, 32, 2, "hybrid")
+    budget = 2 * S.estimate_bytes(small)
+    srv = S.Server(dev, budget_bytes=budget)
+    got = srv.serve([small, huge, S.Request(2, 0.01, 8, 4, 3, "exact")])
+    assert got[0].error is None and got[2].error is None
+    assert got[1].error is not None and "budget" in got[1].error   # host-side admission failure
+    assert srv.stats["rejected"] == 1 and srv.resident_bytes <= budget
+    assert got[0].value == S.answer_alone(small, dev).value
