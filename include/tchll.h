@@ -190,6 +190,24 @@ int tchll_build_sketches_compact(const int32_t* row_ptr, int64_t n_nodes, const 
                                  const int64_t* keys, int64_t nnz, const int64_t* slot, int64_t n_rows, int32_t p,
                                  uint8_t* rows, void* stream);
 
+/*
+ * The cpu_exp estimator variant (cpu_exp/triangle_hll_experiment.py), for
+ * comparison with the reference's published CPU numbers:
+ * tchll_cx_build_registers fills dense rows for EVERY vertex with the seeded
+ * hash h = splitmix64(x + seed + 0x9E3779B97F4A7C15), index = low p bits,
+ * rank from h >> p (:386-401), and sets has_all[u] = 1; tchll_cx_hybrid_count
+ * routes an edge to exact iff min(d+u, d+v) <= threshold (threshold < 0: all
+ * edges HLL, the pure-HLL count) and estimates with estimate_hll_cardinality
+ * (linear counting, else the 2^32 correction; :357-366).  regs must be zeroed
+ * by the caller only for tchll_cx_hybrid_count inputs not made here.
+ */
+int tchll_cx_build_registers(const int32_t* row_ptr, int64_t n_nodes, const int32_t* col_idx, int64_t nnz, int32_t p,
+                             uint64_t seed, uint8_t* regs, uint8_t* has_all, void* stream);
+int tchll_cx_hybrid_count(const int32_t* row_ptr, int64_t n_nodes, const int32_t* col_idx, int64_t nnz,
+                          const int32_t* edge_u, const int32_t* edge_v, int64_t n_edges, const int32_t* degrees,
+                          const uint8_t* regs, const uint8_t* has_all, int32_t p, int64_t threshold,
+                          tchll_count_result* result, void* workspace, size_t workspace_bytes, void* stream);
+
 /* HLL.add_array (src/hll.py:93-96): max-merge the registers of n int64 values
  * into one row of 2^p registers. */
 int tchll_hll_add(uint8_t* regs, int32_t p, const int64_t* values, int64_t n, void* stream);

@@ -410,3 +410,31 @@ def test_device_edge_text_parse(tchll, tmp_path):
         ingest.parse_edge_text(b"1 x\n")
     g = ingest.load_graph(str(p))
     assert g.n_edges == 4 and g.n_nodes == 4
+
+
+# --------------------------------------------------- cpu_exp estimator variant
+def test_cpu_exp_variant_vs_golden(tchll, golden):
+    """Registers and hybrid / pure-HLL tuples of the cpu_exp variant against
+    the outputs recorded from cpu_exp/triangle_hll_experiment.py itself."""
+    import torch
+    from triangle_counting_hll_b200 import core, variants
+    arrays, meta = golden
+    dev = torch.device("cuda", 0)
+    for key, ref in meta["cpu_exp"].items():
+        p = int(key.rsplit("_p", 1)[1])
+        off = arrays[f"cx_{key}_offsets"].astype(np.int32)
+        adj = arrays[f"cx_{key}_adj"].astype(np.int32)
+        e = arrays[f"cx_{key}_edges"].reshape(-1, 2).astype(np.int32)
+        od = arrays[f"cx_{key}_outdeg"].astype(np.int32)
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+        g = core.DeviceCSR(t(off), t(adj), t(od), t(np.arange(len(od), dtype=np.int32)), t(e[:, 0]), t(e[:, 1]))
+        regs, has = variants.cx_build_registers(g, p, seed=1)
+        assert np.array_equal(regs.cpu().numpy()[: len(od) << p], arrays[f"cx_{key}_regs"]), key
+        for thr in ("0", "4", "16", "1000000000"):
+            got = variants.cx_hybrid_count(g, regs, has, p, int(thr))
+            exp = ref[thr]
+            assert (got[1], got[2], got[5]) == (int(exp[1]), int(exp[2]), int(exp[5])), (key, thr)
+            assert got[0] == pytest.approx(exp[0], rel=HYB_RTOL, abs=1e-9), (key, thr)
+            assert got[3] == exp[3]
+        tot, cl = variants.pure_hll_count(g, regs, has, p)
+        assert tot == pytest.approx(ref["pure"][0], rel=HYB_RTOL) and cl == ref["pure"][1]

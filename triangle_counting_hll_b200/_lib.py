@@ -78,6 +78,8 @@ SIGNATURES = {
     "tchll_hll_add": (C.c_int, [_P, _I32, _P, _I64, _P]),
     "tchll_hll_estimate_pairs": (C.c_int, [_P, _I64, _I32, _P, _P, _I64, _P, _P]),
     "tchll_hash64": (C.c_int, [_P, _I64, _P, _P]),
+    "tchll_cx_build_registers": (C.c_int, [_P, _I64, _P, _I64, _I32, _U64, _P, _P, _P]),
+    "tchll_cx_hybrid_count": (C.c_int, [_P, _I64, _P, _I64, _P, _P, _I64, _P, _P, _P, _I32, _I64, _P, _P, _SZ, _P]),
     "tchll_csr_workspace_bytes": (C.c_int, [_I64, C.POINTER(_SZ)]),
     "tchll_csr_build_phase1": (C.c_int, [_P, _P, _I64, _P, _P, _SZ, _P]),
     "tchll_csr_build_phase2": (C.c_int, [_I64, _I64, _I64, _P, _P, _P, _P, _P, _P, _P, _P, _SZ, _P]),

@@ -82,6 +82,17 @@ __device__ __forceinline__ void hll_index_rank(uint64_t x, int p, uint32_t& j, u
     rho = (uint32_t)(rem - (64 - __clzll(w)) + 1);
 }
 
+// The cpu_exp estimator variant (cpu_exp/triangle_hll_experiment.py:369-381,
+// 386-401): h = splitmix64(x + seed) with the +0x9E3779B97F4A7C15 increment,
+// index = low p bits, rank from h >> p (bit_length rule as above).
+__device__ __forceinline__ void hll_index_rank_cx(uint64_t x, uint64_t seed, int p, uint32_t& j, uint32_t& rho) {
+    const int bits = 64 - p;
+    const uint64_t h = splitmix64_fin(x + seed + 0x9E3779B97F4A7C15ull);
+    j = (uint32_t)(h & ((1ull << p) - 1ull));
+    const uint64_t w = h >> p;
+    rho = (uint32_t)(bits - (64 - __clzll(w)) + 1);
+}
+
 // Byte-wise max into a shared-memory register row stored as 32-bit words.
 __device__ __forceinline__ void smem_byte_max(uint32_t* words, uint32_t j, uint32_t rho) {
     uint32_t* w = words + (j >> 2);

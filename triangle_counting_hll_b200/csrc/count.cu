@@ -69,6 +69,7 @@ struct CountParams {
     const uint8_t* has;          // dense layout: has_sketch[v] == 1 -> row v
     int p;
     int64_t gamma;
+    int variant;          // HLL estimator: 0 the reference's src/hll.py, 1 cpu_exp's
     int64_t* pe_support;  // per-edge exact support (details), zeroed by host
     double* pe_s_hat;     // per-edge HLL s_hat (details)
     double* pe_s_cl;      // per-edge HLL clamped support (details)
@@ -533,7 +534,7 @@ __global__ void __launch_bounds__(256, 1) count_kernel(const CountParams P) {
                     const int32_t jdv = __shfl_sync(FULL, dv, j);
                     const uint8_t* ra = P.regs + su * (int64_t)m;
                     const uint8_t* rb = P.regs + sv * (int64_t)m;
-                    const double E = warp_union_estimate<VEC>(ra, rb, P.p, lane);
+                    const double E = warp_union_estimate<VEC>(ra, rb, P.p, lane, P.variant);
                     if (lane == 0) {
                         const double s_hat = (double)((int64_t)jdu + (int64_t)jdv) - E;
                         const double upper = (double)(jdu < jdv ? jdu : jdv);
@@ -1245,4 +1246,36 @@ TCHLL_EXPORT int tchll_batch_hybrid_count(const int32_t* row_ptr, int64_t n_node
     P.gamma = gamma;
     P.result = results;
     return run_batch(P, true, graph_vbase, n_graphs, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+// cpu_exp estimator variant (cpu_exp/triangle_hll_experiment.py:466-498,
+// 652-710): dense registers for every vertex; an edge is exact iff
+// min(d+u, d+v) <= threshold (threshold < 0: every edge HLL, the pure-HLL
+// count).  Same kernels as the hybrid with gamma = threshold + 1.
+TCHLL_EXPORT int tchll_cx_hybrid_count(const int32_t* row_ptr, int64_t n_nodes, const int32_t* col_idx, int64_t nnz,
+                                       const int32_t* edge_u, const int32_t* edge_v, int64_t n_edges,
+                                       const int32_t* degrees, const uint8_t* regs, const uint8_t* has_all,
+                                       int32_t p, int64_t threshold, tchll_count_result* result, void* workspace,
+                                       size_t workspace_bytes, void* stream) {
+    int rc = check_common(row_ptr, n_nodes, col_idx, nnz, edge_u, edge_v, n_edges, result);
+    if (rc) return rc;
+    TCHLL_ARG(p >= 4 && p <= 16, "p must be in [4, 16], got %d", p);
+    TCHLL_ARG(n_edges == 0 || (degrees && regs && has_all), "null degrees / registers");
+    CountParams P{};
+    P.row_ptr = row_ptr;
+    P.n_nodes = n_nodes;
+    P.col_idx = col_idx;
+    P.nnz = nnz;
+    P.edge_u = edge_u;
+    P.edge_v = edge_v;
+    P.n_edges = n_edges;
+    P.degrees = degrees;
+    P.regs = regs;
+    P.n_rows = n_nodes;
+    P.has = has_all;
+    P.p = p;
+    P.gamma = threshold < 0 ? 0 : threshold + 1;
+    P.variant = 1;
+    P.result = result;
+    return run_count(P, 2, false, workspace, workspace_bytes, (cudaStream_t)stream);
 }

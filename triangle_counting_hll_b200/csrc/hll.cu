@@ -144,7 +144,7 @@ __global__ void estimate_pairs_kernel(const uint8_t* rows, int64_t n_rows, int p
             if (lane == 0) out[i] = __longlong_as_double(0x7FF8000000000000ll);  // NaN: bad row index
             continue;
         }
-        const double E = warp_union_estimate<VEC>(rows + sa * m, rows + sb * m, p, lane);
+        const double E = warp_union_estimate<VEC>(rows + sa * m, rows + sb * m, p, lane, 0);
         if (lane == 0) out[i] = E;
     }
 }
@@ -285,5 +285,41 @@ TCHLL_EXPORT int tchll_hash64(const int64_t* values, int64_t n, uint64_t* out, v
     if (n == 0) return TCHLL_OK;
     hash_kernel<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(values, n, out);
     TCHLL_CHECK_LAUNCH("hash_kernel");
+    return TCHLL_OK;
+}
+
+// cpu_exp register build (cpu_exp/triangle_hll_experiment.py:386-401,
+// 526-540): dense rows for every vertex, seeded hash, low-p index; has_all[u]
+// is set to 1 for every u (every vertex carries a sketch in that variant).
+__global__ void cx_registers_kernel(const int32_t* __restrict__ row_ptr, int64_t n, const int32_t* __restrict__ col_idx,
+                                    int64_t nnz, int p, uint64_t seed, uint8_t* regs, uint8_t* has_all) {
+    const int lane = threadIdx.x & 31;
+    const int64_t m = 1ll << p;
+    for (int64_t u = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; u < n;
+         u += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const int32_t rs = row_ptr[u], re = row_ptr[u + 1];
+        if (lane == 0) has_all[u] = 1;
+        if (rs < 0 || re < rs || (int64_t)re > nnz) continue;
+        uint32_t* row = reinterpret_cast<uint32_t*>(regs + u * m);
+        for (int32_t k = rs + lane; k < re; k += 32) {
+            uint32_t j, rho;
+            hll_index_rank_cx((uint64_t)(int64_t)col_idx[k], seed, p, j, rho);
+            global_byte_max(row, j, rho);
+        }
+    }
+}
+
+TCHLL_EXPORT int tchll_cx_build_registers(const int32_t* row_ptr, int64_t n_nodes, const int32_t* col_idx,
+                                          int64_t nnz, int32_t p, uint64_t seed, uint8_t* regs, uint8_t* has_all,
+                                          void* stream) {
+    TCHLL_ARG(p >= 4 && p <= 16, "p must be in [4, 16], got %d", p);
+    TCHLL_ARG(n_nodes >= 0 && (n_nodes == 0 || (row_ptr && regs && has_all)), "bad arguments");
+    TCHLL_ARG(((uintptr_t)regs & 3) == 0, "regs must be 4-byte aligned");
+    if (n_nodes == 0) return TCHLL_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    TCHLL_CUDA(cudaMemsetAsync(regs, 0, (size_t)n_nodes << p, st));
+    cx_registers_kernel<<<grid_for(n_nodes * 32, 256), 256, 0, st>>>(row_ptr, n_nodes, col_idx, nnz, p, seed, regs,
+                                                                     has_all);
+    TCHLL_CHECK_LAUNCH("cx_registers_kernel");
     return TCHLL_OK;
 }

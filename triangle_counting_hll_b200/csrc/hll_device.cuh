@@ -31,8 +31,12 @@ __device__ __forceinline__ void hll_word(uint32_t w, int S, HllPartial& hp) {
 
 // Union estimate for two register rows; every lane returns the same value.
 template <bool VEC>
+// variant 0: src/hll.py:37-54 (linear counting, then the 2^64 correction on
+// the result); variant 1: cpu_exp's estimate_hll_cardinality
+// (cpu_exp/triangle_hll_experiment.py:357-366: linear counting, else the
+// 2^32 correction on the raw estimate).
 __device__ __forceinline__ double warp_union_estimate(const uint8_t* ra, const uint8_t* rb, int p, int lane,
-                                                      uint32_t* zeros_out = nullptr) {
+                                                      int variant = 0, uint32_t* zeros_out = nullptr) {
     const int m = 1 << p;
     const int S = 65 - p;
     HllPartial hp;
@@ -80,12 +84,18 @@ __device__ __forceinline__ double warp_union_estimate(const uint8_t* ra, const u
     else if (m == 64) alpha = 0.709;
     else alpha = 0.7213 / (1.0 + 1.079 / (double)m);
     double E = alpha * (double)m * (double)m / Z;
+    if (zeros_out) *zeros_out = zeros;
+    if (variant == 1) {
+        if (E <= 2.5 * (double)m && zeros > 0) return (double)m * log((double)m / (double)zeros);
+        const double two32 = 4294967296.0;
+        if (E > two32 / 30.0) return -two32 * log(1.0 - E / two32);
+        return E;
+    }
     if (E <= 2.5 * (double)m) {
         if (zeros > 0) E = (double)m * log((double)m / (double)zeros);
     }
     const double two64 = 18446744073709551616.0;
     if (E > two64 / 30.0) E = -two64 * log(1.0 - E / two64);
-    if (zeros_out) *zeros_out = zeros;
     return E;
 }
 

@@ -30,8 +30,8 @@ def parse_edge_text(data: Union[bytes, bytearray, memoryview, np.ndarray, torch.
     if isinstance(data, torch.Tensor):
         text = data.to(device=dev, dtype=torch.uint8).contiguous()
     else:
-        arr = np.frombuffer(bytes(data), dtype=np.uint8) if not isinstance(data, np.ndarray) else data.astype(np.uint8)
-        text = torch.from_numpy(np.ascontiguousarray(arr)).to(dev)
+        arr = np.frombuffer(bytearray(data), dtype=np.uint8) if not isinstance(data, np.ndarray) else data
+        text = torch.from_numpy(np.array(arr, dtype=np.uint8, copy=True)).to(dev)
     n = int(text.numel())
     L = load()
     nb = C.c_size_t(0)
