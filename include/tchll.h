@@ -71,7 +71,8 @@ uint64_t tchll_launch_count(void);
 
 /* --------------------------------------------- exact / hybrid counting --- */
 /* Workspace for tchll_exact_count / tchll_hybrid_count_* on a CSR of n_nodes
- * rows and n_edges edges (holds the reoriented pair list: 8 bytes per edge). */
+ * rows and n_edges edges (the reoriented pair list and, for hybrid counts,
+ * the HLL edge list: 16 bytes per edge + 8 per vertex). */
 int tchll_count_workspace_bytes(int64_t n_nodes, int64_t n_edges, size_t* bytes);
 
 /*

@@ -88,6 +88,10 @@ struct CountParams {
     const int32_t* chunk_graph;
     const int64_t* n_chunks_dev;
     const int32_t* graph_vbase;  // vertex range of graph g: [vbase[g], vbase[g+1])
+    // Hybrid with pairs: the routing pass appends HLL edges here
+    int32_t* hll_u;
+    int32_t* hll_v;
+    unsigned long long* hll_n;
 };
 
 // Bucketized cuckoo table: 2^lgb buckets of two int32 slots (one 8-byte
@@ -207,12 +211,41 @@ __device__ __forceinline__ bool pair_of(const CountParams& P, int64_t e, int32_t
 template <bool HYB>
 __global__ void pair_hist_kernel(const CountParams P, int32_t* cnt) {
     uint32_t status = 0;
+    unsigned long long fallback = 0;
+    const int lane = threadIdx.x & 31;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < P.n_edges;
          e += (int64_t)gridDim.x * blockDim.x) {
-        int32_t x, y;
-        if (pair_of<HYB>(P, e, x, y, status)) atomicAdd(cnt + x, 1);
+        int32_t u, v, us, ue, vs, ve;
+        bool ok = load_edge(P, e, u, v, us, ue, vs, ve, status);
+        bool hll = false;
+        if (HYB && ok) {
+            int32_t du, dv;
+            int64_t su, sv;
+            bool wants, both;
+            ok = route(P, u, v, du, dv, su, sv, wants, both, status);
+            hll = ok && wants && both;
+            fallback += (ok && wants && !both);
+        }
+        if (ok && !hll) atomicAdd(cnt + (((ue - us) >= (ve - vs)) ? u : v), 1);
+        if (HYB && P.hll_u) {
+            // warp-aggregated append of the HLL-routed edges
+            const unsigned act = __activemask();
+            const unsigned bal = __ballot_sync(act, hll);
+            if (bal) {
+                const int leader = __ffs(act) - 1;
+                unsigned long long base = 0;
+                if (lane == leader) base = atomicAdd(P.hll_n, (unsigned long long)__popc(bal));
+                base = __shfl_sync(act, base, leader);
+                if (hll) {
+                    const unsigned long long pos = base + __popc(bal & ((1u << lane) - 1u));
+                    P.hll_u[pos] = u;
+                    P.hll_v[pos] = v;
+                }
+            }
+        }
     }
     if (status) atomicOr(&P.result->status, status);
+    if (HYB && P.hll_u && fallback) atomicAdd((unsigned long long*)&P.result->n_fallback, fallback);
 }
 
 template <bool HYB>
@@ -271,6 +304,7 @@ __device__ __forceinline__ void publish(tchll_count_result* R, uint64_t acc, U12
                                         int64_t n_exact, int64_t n_fallback, int64_t n_clamped, uint32_t status,
                                         int lane) {
     acc = warp_sum_u64(acc);
+    hacc = warp_sum_u128(hacc);  // sub-warp HLL groups each hold their own sum
     n_approx = warp_sum_i64(n_approx);
     n_exact = warp_sum_i64(n_exact);
     n_fallback = warp_sum_i64(n_fallback);
@@ -568,6 +602,143 @@ __global__ void __launch_bounds__(256, 1) count_kernel(const CountParams P) {
     if (!P.chunk_start) publish(P.result, acc, hacc, n_approx, n_exact, n_fallback, n_clamped, status, lane);
 }
 
+// ------------------------------------------------------ HLL edge list ------
+// One group of L lanes per HLL edge (L = min(32, 2^p / 16): p = 8 runs two
+// edges per warp, p >= 9 a warp per edge), the group's lanes striding over
+// the two 2^p-byte rows with 16-byte loads.  Pass 1 counts the zero
+// registers V of the merged row (zero bytes of row_u | row_v).  Every zero
+// register adds exactly 1 to Z = sum 2^-r, so V >= lc_min (the smallest V
+// with alpha*m^2/V <= 2.5m, with a 1e-9 margin for the FP64 comparison) proves
+// the estimator takes its linear-counting branch: E = m * ln(m / V), the same
+// expression the full estimator evaluates, and Z is not needed.  Otherwise
+// pass 2 forms Z exactly (128-bit fixed point) and applies the full
+// estimator.
+struct HllParams {
+    const int32_t* hu;
+    const int32_t* hv;
+    const unsigned long long* n_dev;
+    const int32_t* degrees;
+    const uint8_t* regs;
+    const int64_t* slot;  // null: dense rows (row v at v * 2^p)
+    int p;
+    int variant;
+    uint32_t lc_min;
+    tchll_count_result* result;
+};
+
+__device__ __forceinline__ uint32_t zero_bytes(uint32_t w) { return __popc(__vcmpeq4(w, 0u)) >> 3; }
+
+template <int L>
+__device__ __forceinline__ uint32_t group_sum_u32(uint32_t x, unsigned gmask) {
+#pragma unroll
+    for (int o = L / 2; o > 0; o >>= 1) x += __shfl_xor_sync(gmask, x, o);
+    return x;
+}
+
+template <int L>
+__device__ __forceinline__ U128 group_sum_u128(U128 v, unsigned gmask) {
+#pragma unroll
+    for (int o = L / 2; o > 0; o >>= 1) {
+        U128 t;
+        t.lo = __shfl_xor_sync(gmask, v.lo, o);
+        t.hi = __shfl_xor_sync(gmask, v.hi, o);
+        v.add(t);
+    }
+    return v;
+}
+
+__device__ __forceinline__ void hll_word128(uint32_t w, int S, U128& sum, double& extra) {
+    if (w == 0u) return;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const uint32_t r = (w >> (8 * k)) & 0xFFu;
+        if (r != 0u) {
+            if ((int)r <= S) sum.add(1ull << (S - (int)r));
+            else extra += ldexp(1.0, S - (int)r);
+        }
+    }
+}
+
+template <int L>
+__global__ void __launch_bounds__(256) hll_edges_kernel(const HllParams H) {
+    const int lane = threadIdx.x & 31;
+    const int sub = lane & (L - 1);
+    const unsigned gmask = (L == 32) ? FULL : (((1u << L) - 1u) << (lane & ~(L - 1)));
+    const int64_t gid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / L;
+    const int64_t ngroups = ((int64_t)gridDim.x * blockDim.x) / L;
+    const int64_t n = (int64_t)*H.n_dev;
+    const int m = 1 << H.p;
+    const int nvec = m >> 4;
+    const int S = 65 - H.p;
+    U128 hacc;
+    int64_t n_approx = 0, n_clamped = 0;
+    for (int64_t e = gid; e < n; e += ngroups) {
+        const int32_t u = __ldg(H.hu + e), v = __ldg(H.hv + e);
+        const int64_t su = H.slot ? __ldg(H.slot + u) : (int64_t)u;
+        const int64_t sv = H.slot ? __ldg(H.slot + v) : (int64_t)v;
+        const uint4* a4 = reinterpret_cast<const uint4*>(H.regs + su * (int64_t)m);
+        const uint4* b4 = reinterpret_cast<const uint4*>(H.regs + sv * (int64_t)m);
+        uint32_t zeros = 0;
+#pragma unroll 4
+        for (int i = sub; i < nvec; i += L) {
+            const uint4 a = __ldg(a4 + i), b = __ldg(b4 + i);
+            zeros += zero_bytes(a.x | b.x) + zero_bytes(a.y | b.y) + zero_bytes(a.z | b.z) + zero_bytes(a.w | b.w);
+        }
+        zeros = group_sum_u32<L>(zeros, gmask);
+        double E;
+        if (zeros >= H.lc_min) {
+            E = (double)m * log((double)m / (double)zeros);
+        } else {
+            U128 sum;
+            double extra = 0.0;
+#pragma unroll 2
+            for (int i = sub; i < nvec; i += L) {
+                const uint4 a = __ldg(a4 + i), b = __ldg(b4 + i);
+                hll_word128(__vmaxu4(a.x, b.x), S, sum, extra);
+                hll_word128(__vmaxu4(a.y, b.y), S, sum, extra);
+                hll_word128(__vmaxu4(a.z, b.z), S, sum, extra);
+                hll_word128(__vmaxu4(a.w, b.w), S, sum, extra);
+            }
+            sum = group_sum_u128<L>(sum, gmask);
+#pragma unroll
+            for (int o = L / 2; o > 0; o >>= 1) extra += __shfl_xor_sync(gmask, extra, o);
+            U128 z;
+            z.lo = (uint64_t)zeros << S;
+            z.hi = (uint64_t)zeros >> (64 - S);
+            sum.add(z);
+            const double Z = ldexp(u128_to_double(sum.lo, sum.hi) + extra, -S);
+            double alpha;
+            if (m == 16) alpha = 0.673;
+            else if (m == 32) alpha = 0.697;
+            else if (m == 64) alpha = 0.709;
+            else alpha = 0.7213 / (1.0 + 1.079 / (double)m);
+            E = alpha * (double)m * (double)m / Z;
+            if (H.variant == 1) {
+                if (E <= 2.5 * (double)m && zeros > 0) E = (double)m * log((double)m / (double)zeros);
+                else if (E > 4294967296.0 / 30.0) E = -4294967296.0 * log(1.0 - E / 4294967296.0);
+            } else {
+                if (E <= 2.5 * (double)m) {
+                    if (zeros > 0) E = (double)m * log((double)m / (double)zeros);
+                }
+                const double two64 = 18446744073709551616.0;
+                if (E > two64 / 30.0) E = -two64 * log(1.0 - E / two64);
+            }
+        }
+        if (sub == 0) {
+            const int32_t du = __ldg(H.degrees + u), dv = __ldg(H.degrees + v);
+            const double s_hat = (double)((int64_t)du + (int64_t)dv) - E;
+            const double upper = (double)(du < dv ? du : dv);
+            // max(0.0, min(s_hat, upper)) with Python's min/max argument order
+            double s_cl = (upper < s_hat) ? upper : s_hat;
+            s_cl = (s_cl > 0.0) ? s_cl : 0.0;
+            if (s_hat < 0.0 || s_hat > upper) ++n_clamped;
+            ++n_approx;
+            hacc.add((uint64_t)__double2ull_rn(s_cl * 4294967296.0));
+        }
+    }
+    publish(H.result, 0, hacc, n_approx, 0, 0, n_clamped, 0u, lane);
+}
+
 // ---------------------------------------------------------------- host ------
 struct Tuning {
     int chunk = 256;
@@ -655,6 +826,71 @@ static bool carve_count(void* ws, size_t bytes, int64_t n_nodes, int64_t n_edges
     return cv.ok();
 }
 
+// Hybrid calls also hold the HLL edge list (8 bytes per edge) after the
+// exact-count layout; exact-only calls use the prefix.
+struct HybridWs {
+    int32_t* hll_u;
+    int32_t* hll_v;
+    unsigned long long* hll_n;
+};
+
+static bool carve_count_hybrid(void* ws, size_t bytes, int64_t n_nodes, int64_t n_edges, CountWs& W, HybridWs& H,
+                               size_t* need) {
+    size_t base = 0;
+    carve_count(nullptr, 0, n_nodes, n_edges, W, &base);
+    const size_t E = (size_t)(n_edges > 0 ? n_edges : 1);
+    Carve cv(ws, bytes);
+    char* b = cv.take<char>(base);
+    H.hll_u = cv.take<int32_t>(E);
+    H.hll_v = cv.take<int32_t>(E);
+    H.hll_n = cv.take<unsigned long long>(1);
+    if (need) *need = cv.off;
+    if (!cv.ok()) return false;
+    if (!cv.dry) carve_count(b, base, n_nodes, n_edges, W, nullptr);
+    return true;
+}
+
+static uint32_t lc_min_for(int p) {
+    const double m = (double)(1 << p);
+    double alpha;
+    if (p == 4) alpha = 0.673;
+    else if (p == 5) alpha = 0.697;
+    else if (p == 6) alpha = 0.709;
+    else alpha = 0.7213 / (1.0 + 1.079 / m);
+    return (uint32_t)ceil(alpha * m / 2.5 * (1.0 + 1e-9));
+}
+
+template <int L>
+static int launch_hll_edges_L(const HllParams& H, cudaStream_t st) {
+    const int grid = sm_count() * 8;
+    hll_edges_kernel<L><<<grid, 256, 0, st>>>(H);
+    TCHLL_CHECK_LAUNCH("hll_edges_kernel");
+    return TCHLL_OK;
+}
+
+static int launch_hll_edges(const CountParams& P, const HybridWs& HW, cudaStream_t st) {
+    HllParams H;
+    H.hu = HW.hll_u;
+    H.hv = HW.hll_v;
+    H.n_dev = HW.hll_n;
+    H.degrees = P.degrees;
+    H.regs = P.regs;
+    H.slot = P.slot;
+    H.p = P.p;
+    H.variant = P.variant;
+    H.lc_min = lc_min_for(P.p);
+    H.result = P.result;
+    const int nvec = (1 << P.p) >> 4;
+    switch (nvec >= 32 ? 32 : nvec) {
+        case 1: return launch_hll_edges_L<1>(H, st);
+        case 2: return launch_hll_edges_L<2>(H, st);
+        case 4: return launch_hll_edges_L<4>(H, st);
+        case 8: return launch_hll_edges_L<8>(H, st);
+        case 16: return launch_hll_edges_L<16>(H, st);
+        default: return launch_hll_edges_L<32>(H, st);
+    }
+}
+
 static int grid_edges(int64_t n) {
     int64_t g = (n + 255) / 256;
     const int64_t cap = (int64_t)sm_count() * 16;
@@ -699,8 +935,11 @@ static int build_pairs(const CountParams& P, const CountWs& W, CountParams& Q, c
 
 static int run_count(CountParams P, int mode, bool details, void* ws, size_t ws_bytes, cudaStream_t st) {
     CountWs W;
+    HybridWs HW{};
     size_t need = 0;
-    if (!carve_count(ws, ws_bytes, P.n_nodes, P.n_edges, W, &need) || ws == nullptr) {
+    const bool ok = (mode == MODE_EXACT) ? carve_count(ws, ws_bytes, P.n_nodes, P.n_edges, W, &need)
+                                         : carve_count_hybrid(ws, ws_bytes, P.n_nodes, P.n_edges, W, HW, &need);
+    if (!ok || ws == nullptr) {
         set_error("workspace too small: need %zu bytes, have %zu", need, ws_bytes);
         return TCHLL_EWORKSPACE;
     }
@@ -713,6 +952,9 @@ static int run_count(CountParams P, int mode, bool details, void* ws, size_t ws_
     P.tiny = g_tuning.tiny;
     P.sparse = g_tuning.sparse;
     P.n_edges_dev = nullptr;
+    P.hll_u = nullptr;
+    P.hll_v = nullptr;
+    P.hll_n = nullptr;
     if (P.n_edges == 0) return TCHLL_OK;
     const bool pairs = g_tuning.pairs && !details;
     int rc;
@@ -744,20 +986,28 @@ static int run_count(CountParams P, int mode, bool details, void* ws, size_t ws_
             g_phase.used[1] = true;
             return rc;
         case 2:  // split: exact-routed edges, then HLL-routed edges
-            if (pairs) {
-                // The pair launch adds the exact supports and counts n_exact;
-                // the edge-wise HLL launch adds the HLL estimates, n_approx,
-                // n_clamped and n_fallback.
+            if (pairs && ((uintptr_t)P.regs % 16 == 0)) {
+                // One routing pass builds both work lists: the exact pairs
+                // (counted by the pair launch, which also counts n_exact) and
+                // the HLL edge list (estimated by hll_edges_kernel, which
+                // counts n_approx / n_clamped); the routing pass counts
+                // n_fallback.
                 P.work = W.ctr;
+                P.hll_u = HW.hll_u;
+                P.hll_v = HW.hll_v;
+                P.hll_n = HW.hll_n;
+                TCHLL_CUDA(cudaMemsetAsync(HW.hll_n, 0, sizeof(unsigned long long), st));
                 phase_mark(0, st);
-                rc = build_pairs<true>(P, W, Q, st);
+                rc = pairs_hist_scan<true>(P, W, st);
+                if (rc) return rc;
+                rc = pairs_scatter<true>(P, W, Q, st);
                 if (rc) return rc;
                 phase_mark(1, st);
+                Q.hll_u = nullptr;
                 rc = launch_count<MODE_EXACT>(Q, false, st);
                 if (rc) return rc;
                 phase_mark(2, st);
-                P.work = W.ctr + 1;
-                rc = launch_count<MODE_HYB_HLL>(P, false, st);
+                rc = launch_hll_edges(P, HW, st);
                 phase_mark(3, st);
                 g_phase.used[0] = g_phase.used[1] = g_phase.used[2] = true;
                 return rc;
@@ -796,7 +1046,8 @@ using namespace tchll;
 TCHLL_EXPORT int tchll_count_workspace_bytes(int64_t n_nodes, int64_t n_edges, size_t* bytes) {
     TCHLL_ARG(bytes != nullptr && n_nodes >= 0 && n_edges >= 0, "bad arguments");
     CountWs W;
-    carve_count(nullptr, 0, n_nodes, n_edges, W, bytes);
+    HybridWs H;
+    carve_count_hybrid(nullptr, 0, n_nodes, n_edges, W, H, bytes);  // covers the exact-only layout too
     return TCHLL_OK;
 }
 
