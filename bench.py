@@ -51,6 +51,11 @@ def parse_args():
     ap.add_argument("--scale", type=int, default=SCALE)
     ap.add_argument("--no-extras", action="store_true", help="skip the hybrid / batched / serving extras")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU-baseline sample budget")
+    ap.add_argument("--mode", choices=("exact", "hybrid"), default="exact",
+                    help="exact (the headline line) or hybrid: one hybrid count per step with prebuilt compact "
+                         "sketches (theta = gamma)")
+    ap.add_argument("--p", type=int, default=12, help="HLL precision for --mode hybrid")
+    ap.add_argument("--theta", type=int, default=HYB_THETA, help="sketch / route threshold for --mode hybrid")
     ap.add_argument("--sharded", action="store_true",
                     help="N>1: split one graph's edges across ranks (strong scaling) instead of one graph per rank")
     return ap.parse_args()
@@ -178,6 +183,8 @@ def run_ours(args):
     deg = (g.row_ptr[1:] - g.row_ptr[:-1]).long()
     algo_bytes = 16 * g.n_edges + 4 * int((deg[g.edge_u.long()] + deg[g.edge_v.long()]).sum().item())
     res = _lib.count_result_tensor(dev)
+    if args.mode == "hybrid":
+        return run_hybrid_line(args, g, dev, rank, world, barrier, max_over_ranks)
 
     if args.sharded and world > 1:
         from triangle_counting_hll_b200 import dist as D
@@ -300,6 +307,115 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_hybrid_line(args, g, dev, rank, world, barrier, max_over_ranks):
+    """--mode hybrid: one hybrid count (compact sketches built once, before
+    timing; theta = gamma) per step.  Roofline of the dominant phase: the
+    exact-pair count over exact-routed edges (16 + 4 (d+u + d+v) bytes each)
+    or the HLL pass (16 + 2 * 2^p bytes per HLL edge)."""
+    import torch
+    import torch.distributed as dist
+
+    from triangle_counting_hll_b200 import _lib, core
+    p, theta = args.p, args.theta
+    slot, n_rows = core.sketch_slots(g.row_ptr, theta)
+    rows = core.build_sketches_compact_tensors(g.row_ptr, g.col_idx, slot, n_rows, p)
+    deg = g.degrees.long()
+    du, dv = deg[g.edge_u.long()], deg[g.edge_v.long()]
+    hll = torch.minimum(du, dv) >= theta
+    n_hll = int(hll.sum().item())
+    exact_bytes = 16 * (g.n_edges - n_hll) + 4 * int(torch.where(hll, 0, du + dv).sum().item())
+    hll_bytes = n_hll * (16 + 2 * (1 << p))
+    res = _lib.count_result_tensor(dev)
+    ex_res, _ = core.exact_count_tensors(g.row_ptr, g.col_idx, g.edge_u, g.edge_v)
+    exact = core.exact_from_result(ex_res)
+
+    def step():
+        core.hybrid_count_compact_tensors(g.row_ptr, g.col_idx, g.edge_u, g.edge_v, g.degrees, rows, slot, p, theta,
+                                          split_kernels=True, result=res)
+        return core.hybrid_from_result(res)
+
+    for _ in range(max(args.warmup, 0)):
+        step()
+    core.set_phase_timing(True)
+    launches0 = _lib.launch_count()
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    phases = []
+    ev0.record()
+    for _ in range(args.steps):
+        total, r = step()
+        phases.append(core.phase_times())
+    ev1.record()
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    launches = (_lib.launch_count() - launches0) / max(args.steps, 1)
+    core.set_phase_timing(False)
+    ms_step = max_over_ranks(ev0.elapsed_time(ev1)) / args.steps
+    avg = {k: sum((ph[k] or 0.0) for ph in phases) / len(phases) for k in phases[0]}
+
+    # end to end: CSR + compact sketches from pinned host memory each step
+    host = [t.cpu().pin_memory() for t in (g.row_ptr, g.col_idx, g.edge_u, g.edge_v, g.degrees, rows, slot)]
+    h2d = sum(t.numel() * t.element_size() for t in host)
+
+    def e2e_step():
+        d = [t.to(dev, non_blocking=True) for t in host]
+        core.hybrid_count_compact_tensors(*d[:7], p, theta, split_kernels=True, result=res)
+        return core.hybrid_from_result(res)
+
+    for _ in range(max(1, min(args.warmup, 2))):
+        e2e_step()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        t2, _ = e2e_step()
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1)) / args.steps
+    assert t2 == total
+    del host
+
+    peaks = load_peaks()
+    if avg["hll"] > avg["count"]:
+        kname, kms, kbytes = "hll_edges_kernel", avg["hll"], hll_bytes
+    else:
+        kname, kms, kbytes = "count_kernel<exact pairs>", avg["count"], exact_bytes
+    achieved = kbytes / (kms / 1e3) / 1e9
+    traffic = load_traffic(f"rmat{args.scale}_ef16_hybrid_p{p}_{kname.split('<')[0]}")
+    line = {
+        "metric": METRIC, "value": world * g.n_edges / (ms_step / 1e3), "unit": "edges/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32+u8", "data": "synthetic",
+        "config": {"workload": f"rmat{args.scale}_ef16_hybrid_p{p}_theta{theta}",
+                   "graph": f"R-MAT scale {args.scale} ef {EDGE_FACTOR} (a,b,c)=({ABC[0]},{ABC[1]},{ABC[2]}) "
+                            f"seed {SEED}", "n_edges": g.n_edges, "p": p, "theta": theta, "gamma": theta,
+                   "n_sketched": n_rows, "n_hll_edges": n_hll, "exact_triangles": exact,
+                   "l2": "inputs larger than L2", "parallelism": f"replicas x{world}"},
+        "estimate": total, "rel_err": abs(total - exact) / exact if exact else 0.0,
+        "stats": {"n_approx": int(r.n_approx), "n_exact": int(r.n_exact), "n_clamped": int(r.n_clamped)},
+        "phases_ms": avg,
+        "e2e": {"value": world * g.n_edges / (e2e_ms / 1e3), "unit": "edges/s", "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": _lib.RESULT_BYTES},
+        "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peaks["hbm_gbs"],
+                     "peak_source": peaks["source"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                     "kernel_ms": kms, "algorithmic_bytes": kbytes,
+                     "traffic": traffic["bytes_per_launch"] if traffic else None},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def hybrid_sweep(g, exact_count: int, dev) -> dict:
     import torch
 
@@ -333,6 +449,23 @@ def hybrid_sweep(g, exact_count: int, dev) -> dict:
     return out
 
 
+def calibrate_rate(O, rp, ci, eu, ev, cores: int, min_s: float = 1.0) -> float:
+    """Edges/s of the oracle's exact count on strided samples of the oriented
+    edges, grown 4x at a time until one sample runs for at least min_s (thread
+    start-up and tiny samples understate the rate)."""
+    import numpy as np
+    E = len(eu)
+    n = min(E, 4096)
+    while True:
+        sel = np.arange(0, E, max(E // n, 1))
+        t0 = time.perf_counter()
+        O.exact_count(rp, ci, eu[sel], ev[sel], nthreads=cores)
+        dt = time.perf_counter() - t0
+        if dt >= min_s or len(sel) >= E:
+            return len(sel) / max(dt, 1e-9)
+        n = min(E, n * 4 if dt <= 0 else max(n * 2, int(n * min(8.0, 1.5 * min_s / dt))))
+
+
 def cpu_baseline(g, exact_count: int, budget_s: float) -> dict:
     """The oracle (C restatement of the reference's counting loop) timed on a
     strided sample of the same oriented edges, all host threads."""
@@ -347,12 +480,8 @@ def cpu_baseline(g, exact_count: int, budget_s: float) -> dict:
     ev = g.edge_v.cpu().numpy()
     cores = host_cores()
     E = len(eu)
-    probe = max(E // 2000, 1)
-    sel = np.arange(0, E, probe)
-    t0 = time.perf_counter()
-    O.exact_count(rp, ci, eu[sel], ev[sel], nthreads=cores)
-    rate = len(sel) / max(time.perf_counter() - t0, 1e-6)
-    n = int(min(E, max(len(sel), rate * budget_s)))
+    rate = calibrate_rate(O, rp, ci, eu, ev, cores)
+    n = int(min(E, max(1, rate * budget_s)))
     stride = max(E // n, 1)
     sel = np.arange(0, E, stride)
     t0 = time.perf_counter()
@@ -381,10 +510,7 @@ def run_reference(args):
     del u, v
     rp, ci, eu, ev = g["row_ptr"], g["col_idx"], g["edge_u"], g["edge_v"]
     E = len(eu)
-    probe = np.arange(0, E, max(E // 2000, 1))
-    t0 = time.perf_counter()
-    O.exact_count(rp, ci, eu[probe], ev[probe], nthreads=cores)
-    rate = len(probe) / max(time.perf_counter() - t0, 1e-6)
+    rate = calibrate_rate(O, rp, ci, eu, ev, cores)
     stride = max(int(E // max(rate * 3.0, 1.0)), 1)  # about 3 s of CPU work per step
     sel = np.arange(0, E, stride)
     su, sv = eu[sel], ev[sel]

@@ -75,6 +75,15 @@ uint64_t tchll_launch_count(void);
  * the HLL edge list: 16 bytes per edge + 8 per vertex). */
 int tchll_count_workspace_bytes(int64_t n_nodes, int64_t n_edges, size_t* bytes);
 
+/* Workspace for a hybrid count whose sketches are n_rows register rows of
+ * 2^p bytes (compact: the rows of tchll_build_sketches_compact; dense: n_nodes).
+ * Adds the rows' zero-register masks (max(2^p / 8, 16) bytes per row) to the
+ * tchll_count_workspace_bytes size: with them the HLL pass tests the
+ * linear-counting branch from 2^p / 8 bytes per sketch instead of 2^p.  A
+ * hybrid call given only tchll_count_workspace_bytes still runs, reading the
+ * registers; the results are the same either way. */
+int tchll_hybrid_workspace_bytes(int64_t n_nodes, int64_t n_edges, int64_t n_rows, int32_t p, size_t* bytes);
+
 /*
  * Exact count: T = sum over the n_edges edges (edge_u[i], edge_v[i]) of
  * |N+(u) cap N+(v)| with N+(x) = col_idx[row_ptr[x] .. row_ptr[x+1]) (sorted,
@@ -132,6 +141,17 @@ int tchll_set_count_tuning(int32_t chunk, int32_t slots_log2, int32_t tiny, int3
 int tchll_set_count_shape(int32_t warps_per_cta, int32_t pairs);
 int tchll_set_count_table(int32_t sparse);
 int tchll_get_count_tuning(int32_t* out8 /* host */);
+
+/* Hub pairs (pairs layout only, col_idx 16-byte aligned): pairs whose table
+ * side x has d+(x) > threshold are counted by a kernel in which a whole CTA
+ * shares one hash table of N+(x) (load <= 1/16 where 2^table_log2 slots of
+ * shared memory allow), seg_pairs of x's pairs per work unit, unroll 16-byte
+ * probe loads in flight per lane.  threshold 0 turns it off; otherwise
+ * threshold >= 64, seg_pairs in [256, 2^20], table_log2 in [10, 15], unroll 2
+ * or 4.  out4 receives the four values.  Results are identical for every
+ * setting. */
+int tchll_set_count_hub(int32_t threshold, int32_t seg_pairs, int32_t table_log2, int32_t unroll);
+int tchll_get_count_hub(int32_t* out4 /* host */);
 
 /*
  * Allocation-free exact count, for callers that cannot allocate device memory

@@ -190,6 +190,53 @@ def test_tuning_does_not_change_results(tchll, oracle, dev):
     assert len(set(outs[0::2])) == 1 and len(set(outs[1::2])) == 1
 
 
+def test_hub_kernel_settings_match_oracle(tchll, oracle, dev):
+    """The CTA-table kernel for pairs with a long table side: exact counts and
+    split hybrid totals are the same with it off, with every pair above the
+    smallest threshold, with many short segments per x, and with tables too
+    small for the longest lists (binary-search fallback)."""
+    import torch
+    from triangle_counting_hll_b200 import core
+    u, v = core.gen_rmat(15, 16, 0.57, 0.19, 0.19, seed=5, device=dev)
+    iu, iv = np.triu_indices(700, 1)  # plus a 700-clique: forward lists up to 699 long
+    u = torch.cat([u, torch.from_numpy((iu * 37).astype(np.int32)).to(dev)])
+    v = torch.cat([v, torch.from_numpy((iv * 37).astype(np.int32)).to(dev)])
+    g = core.csr_from_edges(u, v)
+    og = _ocsr(oracle, _np(u), _np(v))
+    want = oracle.exact_count(og["row_ptr"], og["col_idx"], og["edge_u"], og["edge_v"])
+    d = np.diff(og["row_ptr"])
+    assert d.max() > 512  # some lists exceed the 2^10-slot table at load 1/2
+    slot, nr = core.sketch_slots(g.row_ptr, 48)
+    rows = core.build_sketches_compact_tensors(g.row_ptr, g.col_idx, slot, nr, 10)
+    base = core.get_count_tuning()
+    hyb = []
+    try:
+        for hub, seg, lg in ((0, 1024, 13), (256, 1024, 13), (64, 256, 13), (64, 256, 10), (100, 5000, 15)):
+            core.set_count_tuning(base["chunk"], base["slots_log2"], base["tiny"], base["blocks_per_sm"], hub=hub,
+                                  hub_seg=seg, hub_lg=lg)
+            assert core.get_count_tuning()["hub"] == hub
+            assert _exact(core, g) == want, (hub, seg, lg)
+            res, _ = core.hybrid_count_compact_tensors(g.row_ptr, g.col_idx, g.edge_u, g.edge_v, g.degrees, rows,
+                                                       slot, 10, 48, split_kernels=True)
+            tot, r = core.hybrid_from_result(res)
+            hyb.append((tot, int(r.exact), int(r.n_exact), int(r.n_approx)))
+            assert int(r.n_exact) + int(r.n_approx) == g.n_edges
+        # unaligned col_idx: the hub path is skipped, the count is unchanged
+        core.set_count_tuning(base["chunk"], base["slots_log2"], base["tiny"], base["blocks_per_sm"], hub=64)
+        col2 = torch.empty(g.col_idx.numel() + 1, dtype=torch.int32, device=dev)
+        col2[1:] = g.col_idx
+        res, _ = core.exact_count_tensors(g.row_ptr, col2[1:], g.edge_u, g.edge_v)
+        assert core.exact_from_result(res) == want
+    finally:
+        core.set_count_tuning(**base)
+    assert len(set(hyb)) == 1
+    with pytest.raises(ValueError):
+        core.set_count_tuning(hub=32)
+    with pytest.raises(ValueError):
+        core.set_count_tuning(hub=256, hub_seg=100)
+    assert core.get_count_tuning()["hub"] == base["hub"]
+
+
 # ---------------------------------------------------------------- sketches
 @pytest.mark.parametrize("p", [4, 8, 10, 12, 14, 16])
 def test_dense_sketches_bit_exact(tchll, oracle, dev, p):
@@ -337,6 +384,55 @@ def test_hybrid_dense_rmat_vs_oracle(tchll, oracle, dev, p):
         assert st["n_approx"] == ost["n_approx"] and st["n_clamped"] == ost["n_clamped"]
         assert st["n_exact"] == ost["n_exact"]
         assert st["kernel_mode"] == ("split_block_reduction" if split else "fused_block_reduction")
+
+
+@pytest.mark.parametrize("p", [4, 6, 8, 10, 12, 16])
+def test_hybrid_zero_masks_give_identical_results(tchll, oracle, dev, p):
+    """The HLL pass with zero-register masks (workspace from
+    tchll_hybrid_workspace_bytes) and without them (the smaller
+    tchll_count_workspace_bytes size) yields byte-identical result blocks,
+    compact and dense, equal to the oracle."""
+    import ctypes as C
+    import torch
+    from triangle_counting_hll_b200 import _lib, core
+    L = _lib.load()
+    u, v = core.gen_rmat(13, 16, 0.57, 0.19, 0.19, seed=7, device=dev)
+    g = core.csr_from_edges(u, v)
+    theta = 12
+    slot, nr = core.sketch_slots(g.row_ptr, theta)
+    rows = core.build_sketches_compact_tensors(g.row_ptr, g.col_idx, slot, nr, p)
+    regs, has = tchll.alloc_sketch_arrays_device(g.n_nodes, p)
+    tchll.build_sketches_kernel[(g.n_nodes + 255) // 256, 256](g.row_ptr, g.col_idx, g.n_nodes, theta, p, regs, has)
+    small, big = C.c_size_t(0), C.c_size_t(0)
+    assert L.tchll_count_workspace_bytes(g.n_nodes, g.n_edges, C.byref(small)) == 0
+    blocks = []
+    for dense in (False, True):
+        n_rows = g.n_nodes if dense else nr
+        assert L.tchll_hybrid_workspace_bytes(g.n_nodes, g.n_edges, n_rows, p, C.byref(big)) == 0
+        assert big.value > small.value
+        for nb in (small.value, big.value):
+            ws = torch.empty(nb, dtype=torch.uint8, device=dev)
+            res = _lib.count_result_tensor(dev)
+            st = _lib.stream_handle(dev)
+            P = _lib.ptr
+            if dense:
+                rc = L.tchll_hybrid_count_dense(P(g.row_ptr), g.n_nodes, P(g.col_idx), g.n_edges, P(g.edge_u),
+                                                P(g.edge_v), g.n_edges, P(g.degrees), P(regs), P(has), p, theta, 1,
+                                                P(res), P(ws), nb, st)
+            else:
+                rc = L.tchll_hybrid_count_compact(P(g.row_ptr), g.n_nodes, P(g.col_idx), g.n_edges, P(g.edge_u),
+                                                  P(g.edge_v), g.n_edges, P(g.degrees), P(rows), nr, P(slot), p,
+                                                  theta, 1, None, None, None, None, P(res), P(ws), nb, st)
+            assert rc == 0, L.tchll_last_error()
+            blocks.append(bytes(_np(res)))
+    assert all(b == blocks[0] for b in blocks)
+    tot, r = core.hybrid_from_result(res)
+    og = _ocsr(oracle, _np(u), _np(v))
+    oregs, ohas = oracle.build_sketches_dense(og["row_ptr"], og["col_idx"], g.n_nodes, theta, p)
+    otot, ost, _ = oracle.hybrid_count(og["row_ptr"], og["col_idx"], og["edge_u"], og["edge_v"], og["degrees"],
+                                       oracle.dense_slots(ohas), oregs, p, theta, nthreads=0)
+    assert int(r.n_approx) == ost["n_approx"] > 0 and int(r.n_clamped) == ost["n_clamped"]
+    assert tot == pytest.approx(otot, rel=HYB_RTOL)
 
 
 def test_hybrid_all_exact_equals_exact(tchll, dev):

@@ -59,6 +59,7 @@ SIGNATURES = {
     "tchll_version": (C.c_int, []),
     "tchll_launch_count": (_U64, []),
     "tchll_count_workspace_bytes": (C.c_int, [_I64, _I64, C.POINTER(_SZ)]),
+    "tchll_hybrid_workspace_bytes": (C.c_int, [_I64, _I64, _I64, C.c_int32, C.POINTER(_SZ)]),
     "tchll_exact_count": (C.c_int, [_P, _I64, _P, _I64, _P, _P, _I64, _P, _P, _P, _SZ, _P]),
     "tchll_hybrid_count_dense": (C.c_int, [_P, _I64, _P, _I64, _P, _P, _I64, _P, _P, _P, _I32, _I64, _I32,
                                            _P, _P, _SZ, _P]),
@@ -68,6 +69,8 @@ SIGNATURES = {
     "tchll_set_count_shape": (C.c_int, [_I32, _I32]),
     "tchll_set_count_table": (C.c_int, [_I32]),
     "tchll_get_count_tuning": (C.c_int, [_P]),
+    "tchll_set_count_hub": (C.c_int, [_I32, _I32, _I32, _I32]),
+    "tchll_get_count_hub": (C.c_int, [_P]),
     "tchll_exact_count_noalloc": (C.c_int, [_P, _I64, _P, _I64, _P, _P, _I64, _P, _P]),
     "tchll_set_phase_timing": (C.c_int, [_I32]),
     "tchll_phase_times": (C.c_int, [_P]),

@@ -175,6 +175,12 @@ def _count_ws(n_nodes: int, n_edges: int, device) -> torch.Tensor:
     return _ws(nb.value, device)
 
 
+def _hybrid_ws(n_nodes: int, n_edges: int, n_rows: int, p: int, device) -> torch.Tensor:
+    nb = C.c_size_t(0)
+    check(load().tchll_hybrid_workspace_bytes(int(n_nodes), int(n_edges), int(n_rows), int(p), C.byref(nb)))
+    return _ws(nb.value, device)
+
+
 def exact_count_tensors(row_ptr: torch.Tensor, col_idx: torch.Tensor, edge_u: torch.Tensor,
                         edge_v: torch.Tensor, per_edge: bool = False,
                         result: Optional[torch.Tensor] = None) -> Tuple[torch.Tensor, Optional[torch.Tensor]]:
@@ -206,7 +212,7 @@ def hybrid_count_dense_tensors(row_ptr, col_idx, edge_u, edge_v, degrees, sketch
     if int(has_sketch.numel()) < n_nodes or int(degrees.numel()) < n_nodes:
         raise ValueError("has_sketch / degrees shorter than n_nodes")
     res = result if result is not None else _lib.count_result_tensor(dev)
-    ws = _count_ws(n_nodes, n_edges, dev)
+    ws = _hybrid_ws(n_nodes, n_edges, n_nodes, p, dev) if m else _count_ws(n_nodes, n_edges, dev)
     check(load().tchll_hybrid_count_dense(ptr(row_ptr), n_nodes, ptr(col_idx), int(col_idx.numel()),
                                           ptr(edge_u), ptr(edge_v), n_edges, ptr(degrees), ptr(sketch_regs),
                                           ptr(has_sketch), int(p), int(gamma), 1 if split_kernels else 0,
@@ -230,7 +236,7 @@ def hybrid_count_compact_tensors(row_ptr, col_idx, edge_u, edge_v, degrees, rows
               torch.empty(n_edges, dtype=torch.float64, device=dev),
               torch.empty(n_edges, dtype=torch.float64, device=dev),
               torch.empty(n_edges, dtype=torch.uint8, device=dev))
-    ws = _count_ws(n_nodes, n_edges, dev)
+    ws = _hybrid_ws(n_nodes, n_edges, n_rows, p, dev) if 4 <= int(p) <= 16 else _count_ws(n_nodes, n_edges, dev)
     pp = [ptr(t) for t in pe] if pe else [None, None, None, None]
     check(load().tchll_hybrid_count_compact(ptr(row_ptr), n_nodes, ptr(col_idx), int(col_idx.numel()),
                                             ptr(edge_u), ptr(edge_v), n_edges, ptr(degrees), ptr(rows), n_rows,
@@ -242,10 +248,18 @@ def hybrid_count_compact_tensors(row_ptr, col_idx, edge_u, edge_v, degrees, rows
 
 def set_count_tuning(chunk: int = 256, slots_log2: int = 11, tiny: int = 16, blocks_per_sm: int = 0,
                      warps: Optional[int] = None, pairs: Optional[bool] = None,
-                     sparse: Optional[bool] = None) -> None:
-    """Launch shape of the counting kernels (results do not depend on it)."""
+                     sparse: Optional[bool] = None, hub: Optional[int] = None, hub_seg: Optional[int] = None,
+                     hub_lg: Optional[int] = None, hub_unroll: Optional[int] = None) -> None:
+    """Launch shape of the counting kernels (results do not depend on it).
+    hub / hub_seg / hub_lg / hub_unroll: threshold on d+(x) above which a pair
+    goes to the CTA-shared table kernel (0: off), pairs per work unit, log2
+    table slots, probe loads in flight per lane."""
     L = load()
     cur = get_count_tuning()
+    check(L.tchll_set_count_hub(int(cur["hub"] if hub is None else hub),
+                                int(cur["hub_seg"] if hub_seg is None else hub_seg),
+                                int(cur["hub_lg"] if hub_lg is None else hub_lg),
+                                int(cur["hub_unroll"] if hub_unroll is None else hub_unroll)))
     check(L.tchll_set_count_table(int(cur["sparse"] if sparse is None else bool(sparse))))
     w = cur["warps"] if warps is None else int(warps)
     pr = cur["pairs"] if pairs is None else int(bool(pairs))
@@ -258,8 +272,11 @@ def set_count_tuning(chunk: int = 256, slots_log2: int = 11, tiny: int = 16, blo
 def get_count_tuning() -> dict:
     out = (C.c_int32 * 8)()
     check(load().tchll_get_count_tuning(C.cast(out, C.c_void_p)))
+    hub = (C.c_int32 * 4)()
+    check(load().tchll_get_count_hub(C.cast(hub, C.c_void_p)))
     return {"chunk": out[0], "slots_log2": out[1], "tiny": out[2], "blocks_per_sm": out[3], "warps": out[4],
-            "pairs": out[5], "sparse": out[6]}
+            "pairs": out[5], "sparse": out[6], "hub": hub[0], "hub_seg": hub[1], "hub_lg": hub[2],
+            "hub_unroll": hub[3]}
 
 
 def set_phase_timing(enable: bool) -> None:

@@ -192,7 +192,8 @@ __device__ __forceinline__ bool route(const CountParams& P, int32_t u, int32_t v
 // Exact edges (all edges, or in hybrid mode the exact-routed ones) become
 // pairs (x, y), x the endpoint with the longer forward list (ties: u).
 template <bool HYB>
-__device__ __forceinline__ bool pair_of(const CountParams& P, int64_t e, int32_t& x, int32_t& y, uint32_t& status) {
+__device__ __forceinline__ bool pair_of(const CountParams& P, int64_t e, int32_t& x, int32_t& y, int32_t& xl,
+                                        uint32_t& status) {
     int32_t u, v, us, ue, vs, ve;
     if (!load_edge(P, e, u, v, us, ue, vs, ve, status)) return false;
     if (HYB) {
@@ -205,6 +206,7 @@ __device__ __forceinline__ bool pair_of(const CountParams& P, int64_t e, int32_t
     const bool ux = (ue - us) >= (ve - vs);
     x = ux ? u : v;
     y = ux ? v : u;
+    xl = ux ? (ue - us) : (ve - vs);
     return true;
 }
 
@@ -248,16 +250,24 @@ __global__ void pair_hist_kernel(const CountParams P, int32_t* cnt) {
     if (HYB && P.hll_u && fallback) atomicAdd((unsigned long long*)&P.result->n_fallback, fallback);
 }
 
+// Small pairs go to [cursor[x]...) of px / py; with hub > 0, pairs whose x
+// has d+(x) > hub go to the hub list, py[*n_small + cursorh[x]...] (y only).
 template <bool HYB>
-__global__ void pair_scatter_kernel(const CountParams P, int32_t* cursor, int32_t* px, int32_t* py) {
+__global__ void pair_scatter_kernel(const CountParams P, int32_t* cursor, int32_t* cursorh, int hub,
+                                    const int32_t* n_small, int32_t* px, int32_t* py) {
     uint32_t status = 0;
+    const int64_t hbase = hub > 0 ? (int64_t)*n_small : 0;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < P.n_edges;
          e += (int64_t)gridDim.x * blockDim.x) {
-        int32_t x, y;
-        if (pair_of<HYB>(P, e, x, y, status)) {
-            const int32_t pos = atomicAdd(cursor + x, 1);
-            px[pos] = x;
-            py[pos] = y;
+        int32_t x, y, xl;
+        if (pair_of<HYB>(P, e, x, y, xl, status)) {
+            if (hub > 0 && xl > hub) {
+                py[hbase + atomicAdd(cursorh + x, 1)] = y;
+            } else {
+                const int32_t pos = atomicAdd(cursor + x, 1);
+                px[pos] = x;
+                py[pos] = y;
+            }
         }
     }
 }
@@ -602,6 +612,284 @@ __global__ void __launch_bounds__(256, 1) count_kernel(const CountParams P) {
     if (!P.chunk_start) publish(P.result, acc, hacc, n_approx, n_exact, n_fallback, n_clamped, status, lane);
 }
 
+// ------------------------------------------------------------ hub pairs ----
+// Pairs whose table side x has a long forward list (d+(x) > hub threshold)
+// carry most of the probe work on skewed graphs (R-MAT scale 22: 90% of the
+// sum of min(d+u, d+v) has d+(x) > 256).  They are counted one x at a time
+// by a whole CTA: the CTA builds ONE table of N+(x) in shared memory at load
+// <= 1/8 (up to 2^hub_lg slots) and its warps stream the probe lists of x's
+// pairs through it.
+//
+// Table: one 4-byte word per slot, bits 0-30 the key (0x7FFFFFFF = empty;
+// vertex ids stay below INT32_MAX) and bit 31 an overflow flag.  A key lives
+// in its home slot h1(k) when that was free at insertion; otherwise it sets
+// the flag on h1(k) and takes the first free slot of a linear walk from
+// h2(k).  A lookup reads the home slot: match -> hit; flag clear -> miss; flag
+// set (about load^2 of the slots) -> walk from h2(k) to the key or a free
+// slot.  So almost every lookup is ONE 4-byte shared load and the warp rarely
+// diverges, against two 8-byte loads for the per-warp cuckoo table.
+struct HubSeg {
+    int64_t start;  // first pair in the hub list
+    int32_t x;
+    int32_t len;
+};
+
+struct HubParams {
+    const int32_t* row_ptr;
+    const int32_t* col_idx;
+    int64_t nnz;
+    const int32_t* hy;  // y of each hub pair, grouped by x
+    const HubSeg* segs;
+    const unsigned long long* n_segs;
+    int64_t max_segs;
+    unsigned long long* seg_ctr;
+    int hub_lg;  // log2 of the largest table (slots)
+    tchll_count_result* result;
+};
+
+constexpr uint32_t OV_KEY = 0x7FFFFFFFu;   // key bits; this value marks an empty slot
+constexpr uint32_t OV_FLAG = 0x80000000u;  // some key of this home slot lives on its h2 walk
+constexpr uint32_t OV_NONE = 0x7FFFFFFEu;  // probe that matches no slot (vertex ids are below it)
+
+__device__ __forceinline__ uint32_t ov_h1(int32_t x, int sh) { return ((uint32_t)x * 0x9E3779B1u) >> sh; }
+__device__ __forceinline__ uint32_t ov_h2(int32_t x, int sh) { return ((uint32_t)x * 0x85EBCA77u) >> sh; }
+
+// Claims slot h for key x if its key bits are empty (keeps the flag bit).
+// Returns 1 placed, 0 occupied by another key, 2 already holds x.
+__device__ __forceinline__ int ov_claim(uint32_t* T, uint32_t h, uint32_t x) {
+    uint32_t old = *(volatile uint32_t*)(T + h);
+    while ((old & OV_KEY) == OV_KEY) {
+        const uint32_t prev = atomicCAS(T + h, old, (old & OV_FLAG) | x);
+        if (prev == old) return 1;
+        old = prev;
+    }
+    return (old & OV_KEY) == x ? 2 : 0;
+}
+
+// Inserts x; false only if the h2 walk finds no free slot (full table).
+__device__ __forceinline__ bool ov_insert(uint32_t* T, int32_t x, int sh, uint32_t mask) {
+    const uint32_t h = ov_h1(x, sh);
+    if (ov_claim(T, h, (uint32_t)x)) return true;
+    atomicOr(T + h, OV_FLAG);
+    uint32_t g = ov_h2(x, sh);
+    for (uint32_t i = 0; i <= mask; ++i) {
+        if (ov_claim(T, g, (uint32_t)x)) return true;
+        g = (g + 1u) & mask;
+    }
+    return false;
+}
+
+// The h2 walk of a lookup whose home slot was flagged: 1 at x, 0 at a free
+// slot; at most mask + 1 steps.
+__device__ __forceinline__ uint32_t ov_walk(const uint32_t* T, int32_t x, int sh, uint32_t mask) {
+    uint32_t g = ov_h2(x, sh);
+    for (uint32_t i = 0; i <= mask; ++i) {
+        const uint32_t k = T[g] & OV_KEY;
+        if (k == (uint32_t)x) return 1u;
+        if (k == OV_KEY) return 0u;
+        g = (g + 1u) & mask;
+    }
+    return 0u;
+}
+
+template <int UNR>
+__global__ void __launch_bounds__(256, 4) hub_count_kernel(const HubParams H) {
+    extern __shared__ __align__(16) uint32_t tbl[];
+    __shared__ HubSeg s_seg;
+    __shared__ int s_round;
+    __shared__ int s_fail;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int32_t* __restrict__ col = H.col_idx;
+    const int64_t nseg = min((int64_t)*H.n_segs, H.max_segs);
+    uint64_t acc = 0;
+    int64_t n_pairs = 0;
+    while (true) {
+        if (tid == 0) {
+            const unsigned long long s = atomicAdd(H.seg_ctr, 1ull);
+            if ((int64_t)s < nseg) {
+                s_seg = H.segs[s];
+            } else {
+                s_seg.x = -1;
+                s_seg.len = 0;
+                s_seg.start = 0;
+            }
+            s_round = 0;
+            s_fail = 0;
+        }
+        __syncthreads();
+        const HubSeg sg = s_seg;
+        if (sg.x < 0) break;
+        if (tid == 0) n_pairs += sg.len;
+        const int32_t xs = __ldg(H.row_ptr + sg.x);
+        const int xl = __ldg(H.row_ptr + sg.x + 1) - xs;
+        int lgs = ceil_log2_i(xl) + 4;  // load <= 1/16 where the cap allows
+        lgs = lgs < 7 ? 7 : (lgs > H.hub_lg ? H.hub_lg : lgs);
+        const uint32_t mask = (1u << lgs) - 1u;
+        const int sh = 32 - lgs;
+        const bool fits = 2 * (int64_t)xl <= (int64_t)(1 << lgs);  // load <= 1/2
+        if (fits) {
+            for (int i = tid; i < (1 << lgs) / 4; i += blockDim.x)
+                reinterpret_cast<uint4*>(tbl)[i] = make_uint4(OV_KEY, OV_KEY, OV_KEY, OV_KEY);
+            __syncthreads();
+            for (int i = tid; i < xl; i += blockDim.x)
+                if (!ov_insert(tbl, __ldg(col + xs + i), sh, mask)) s_fail = 1;
+            __syncthreads();
+        }
+        const bool table = fits && !s_fail;  // CTA-uniform
+        while (true) {
+            int r = 0;
+            if (lane == 0) r = atomicAdd(&s_round, 32);
+            r = __shfl_sync(FULL, r, 0);
+            if (r >= sg.len) break;
+            const int np = min(32, sg.len - r);
+            int32_t vs = 0, ve = 0;
+            if (lane < np) {
+                const int32_t y = __ldg(H.hy + sg.start + r + lane);
+                vs = __ldg(H.row_ptr + y);
+                ve = __ldg(H.row_ptr + y + 1);
+            }
+            if (!table) {  // x's list too long for the table: binary search per pair
+                for (int j = 0; j < np; ++j) {
+                    const int32_t jvs = __shfl_sync(FULL, vs, j);
+                    const int32_t jve = __shfl_sync(FULL, ve, j);
+                    acc += warp_bsearch_count(col + xs, xl, col + jvs, jve - jvs, lane);
+                }
+                continue;
+            }
+            // flatten the 32 probe lists into one stream of 16-byte quads
+            const int q0 = vs >> 2;
+            const int nq = (lane < np && ve > vs) ? ((ve - 1) >> 2) - q0 + 1 : 0;
+            const unsigned ne = __ballot_sync(FULL, nq > 0);
+            const int k = __popc(ne);
+            const int src = lane < k ? (int)__fns(ne, 0, lane + 1) : lane;
+            const int c_q0 = __shfl_sync(FULL, q0, src);
+            int c_nq = __shfl_sync(FULL, nq, src);
+            const int32_t c_vs = __shfl_sync(FULL, vs, src);
+            const int32_t c_ve = __shfl_sync(FULL, ve, src);
+            if (lane >= k) c_nq = 0;
+            int incl = c_nq;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += t;
+            }
+            const int excl = incl - c_nq;
+            const int W = __shfl_sync(FULL, incl, 31);
+            const int qb = c_q0 - excl;
+            for (int T0 = 0; T0 < W; T0 += 32 * UNR) {
+                int qd[UNR], lo[UNR], hi[UNR];
+#pragma unroll
+                for (int i = 0; i < UNR; ++i) {
+                    const int Ti = T0 + 32 * i;
+                    qd[i] = -1;
+                    lo[i] = hi[i] = 0;
+                    if (Ti < W) {  // warp-uniform
+                        const unsigned cover = __ballot_sync(FULL, lane < k && excl <= Ti && Ti < incl);
+                        const int b = __ffs(cover) - 1;
+                        const unsigned bit = (lane < k && excl > Ti && excl < Ti + 32) ? (1u << (excl - Ti)) : 0u;
+                        const unsigned B = __reduce_or_sync(FULL, bit);
+                        const int j = (b + __popc(B & ((2u << lane) - 1u))) & 31;
+                        const int my_qb = __shfl_sync(FULL, qb, j);
+                        const int32_t my_vs = __shfl_sync(FULL, c_vs, j);
+                        const int32_t my_ve = __shfl_sync(FULL, c_ve, j);
+                        if (Ti + lane < W) {
+                            qd[i] = my_qb + Ti + lane;
+                            lo[i] = my_vs - qd[i] * 4;  // valid elements of the quad: [lo, hi)
+                            hi[i] = my_ve - qd[i] * 4;
+                        }
+                    }
+                }
+                int4 val[UNR];
+#pragma unroll
+                for (int i = 0; i < UNR; ++i) {
+                    val[i] = make_int4(-1, -1, -1, -1);
+                    if (qd[i] >= 0) {
+                        const int64_t base = (int64_t)qd[i] * 4;
+                        if (base + 3 < H.nnz) {
+                            val[i] = __ldg(reinterpret_cast<const int4*>(col) + qd[i]);
+                        } else {
+                            val[i].x = base + 0 < H.nnz ? __ldg(col + base + 0) : -1;
+                            val[i].y = base + 1 < H.nnz ? __ldg(col + base + 1) : -1;
+                            val[i].z = base + 2 < H.nnz ? __ldg(col + base + 2) : -1;
+                            val[i].w = base + 3 < H.nnz ? __ldg(col + base + 3) : -1;
+                        }
+                    }
+                }
+                // Home slots of all 4 * UNR keys, branch-free: elements
+                // outside the pair's list (quad edges, idle lanes) probe as
+                // OV_NONE, which matches no slot.  Then the rare walks of
+                // flagged homes.
+                uint32_t key[4 * UNR];
+#pragma unroll
+                for (int i = 0; i < UNR; ++i) {
+                    // lo <= 3 and hi >= 1 for every mapped quad; unmapped: lo = hi = 0
+                    key[4 * i + 0] = (lo[i] <= 0 && hi[i] > 0) ? (uint32_t)val[i].x : OV_NONE;
+                    key[4 * i + 1] = (lo[i] <= 1 && hi[i] > 1) ? (uint32_t)val[i].y : OV_NONE;
+                    key[4 * i + 2] = (lo[i] <= 2 && hi[i] > 2) ? (uint32_t)val[i].z : OV_NONE;
+                    key[4 * i + 3] = (lo[i] <= 3 && hi[i] > 3) ? (uint32_t)val[i].w : OV_NONE;
+                }
+                uint32_t c = 0, pend = 0;
+#pragma unroll
+                for (int t = 0; t < 4 * UNR; ++t) {
+                    const uint32_t d = tbl[ov_h1((int32_t)key[t], sh)] ^ key[t];
+                    c += (d << 1) == 0u;                       // key bits equal
+                    pend |= (d > OV_FLAG ? 1u : 0u) << t;      // flagged home, other key
+                }
+                if (pend) {
+#pragma unroll
+                    for (int t = 0; t < 4 * UNR; ++t)
+                        if ((pend >> t) & 1u) c += ov_walk(tbl, (int32_t)key[t], sh, mask);
+                }
+                acc += c;
+            }
+        }
+        __syncthreads();  // every warp is done with this table
+    }
+    acc = warp_sum_u64(acc);
+    n_pairs = warp_sum_i64(n_pairs);
+    if (lane == 0) {
+        if (acc) atomicAdd((unsigned long long*)&H.result->exact, (unsigned long long)acc);
+        if (n_pairs) atomicAdd((unsigned long long*)&H.result->n_exact, (unsigned long long)n_pairs);
+    }
+}
+
+// Hub segments: x's hub pairs [offh[x], offh[x] + cnth[x]) (shifted by the
+// small-pair total *n_small) cut into pieces of at most seg pairs.
+__global__ void hub_segments_kernel(const int32_t* __restrict__ cnth, const int32_t* __restrict__ offh,
+                                    const int32_t* __restrict__ n_small, int64_t n_nodes, int seg, HubSeg* segs,
+                                    unsigned long long* n_segs, int64_t max_segs) {
+    const int64_t base_pairs = (int64_t)*n_small;
+    for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < n_nodes;
+         x += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t c = __ldg(cnth + x);
+        if (c <= 0) continue;
+        const int k = (c + seg - 1) / seg;
+        const unsigned long long b = atomicAdd(n_segs, (unsigned long long)k);
+        for (int j = 0; j < k; ++j) {
+            if ((int64_t)(b + j) >= max_segs) break;  // cannot happen: sized for the worst case
+            HubSeg s;
+            s.start = base_pairs + __ldg(offh + x) + (int64_t)j * seg;
+            s.x = (int32_t)x;
+            s.len = min(seg, c - j * seg);
+            segs[b + j] = s;
+        }
+    }
+}
+
+// Splits the pair histogram: cnt[x] keeps x's small pairs, cnth[x] gets its
+// hub pairs (all of x's pairs go one way: hub-ness depends on d+(x) only).
+__global__ void hub_split_kernel(const int32_t* __restrict__ row_ptr, int64_t n_nodes, int hub, int32_t* cnt,
+                                 int32_t* cnth) {
+    for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x <= n_nodes;
+         x += (int64_t)gridDim.x * blockDim.x) {
+        int32_t c = cnt[x];
+        bool is_hub = false;
+        if (x < n_nodes && c > 0) is_hub = (__ldg(row_ptr + x + 1) - __ldg(row_ptr + x)) > hub;
+        cnth[x] = is_hub ? c : 0;
+        if (is_hub) cnt[x] = 0;
+    }
+}
+
 // ------------------------------------------------------ HLL edge list ------
 // One group of L lanes per HLL edge (L = min(32, 2^p / 16): p = 8 runs two
 // edges per warp, p >= 9 a warp per edge), the group's lanes striding over
@@ -620,11 +908,44 @@ struct HllParams {
     const int32_t* degrees;
     const uint8_t* regs;
     const int64_t* slot;  // null: dense rows (row v at v * 2^p)
+    const uint32_t* zm;   // zero masks, zst words per row (null: count zeros from the registers)
+    int zst;
     int p;
     int variant;
     uint32_t lc_min;
     tchll_count_result* result;
 };
+
+// Zero-register masks: bit j of word w of row r is set iff register 32w + j
+// of the row is 0.  Rows are zst >= 4 words (16-byte aligned); bits past 2^p
+// stay clear.  One warp per row; dense layouts skip rows without a sketch
+// (no HLL edge reads them).
+__global__ void __launch_bounds__(256) zmask_kernel(const uint8_t* __restrict__ regs, int64_t n_rows,
+                                                    const uint8_t* __restrict__ has, int p, int zst,
+                                                    uint32_t* __restrict__ zm) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int m = 1 << p;
+    for (int64_t r = warp; r < n_rows; r += nwarps) {
+        if (has && !__ldg(has + r)) continue;
+        const uint4* row = reinterpret_cast<const uint4*>(regs + r * (int64_t)m);
+        for (int w = lane; w < zst; w += 32) {
+            uint32_t bits = 0;
+            if (32 * w < m) {
+                const uint4 a = __ldg(row + 2 * w);
+                bits = (__vcmpeq4(a.x, 0u) & 0x01010101u) | ((__vcmpeq4(a.y, 0u) & 0x01010101u) << 1) |
+                       ((__vcmpeq4(a.z, 0u) & 0x01010101u) << 2) | ((__vcmpeq4(a.w, 0u) & 0x01010101u) << 3);
+                if (32 * w + 16 < m) {
+                    const uint4 b = __ldg(row + 2 * w + 1);
+                    bits |= ((__vcmpeq4(b.x, 0u) & 0x01010101u) << 4) | ((__vcmpeq4(b.y, 0u) & 0x01010101u) << 5) |
+                            ((__vcmpeq4(b.z, 0u) & 0x01010101u) << 6) | ((__vcmpeq4(b.w, 0u) & 0x01010101u) << 7);
+                }
+            }
+            zm[r * (int64_t)zst + w] = bits;  // bit order is a permutation of the registers: only popc is used
+        }
+    }
+}
 
 __device__ __forceinline__ uint32_t zero_bytes(uint32_t w) { return __popc(__vcmpeq4(w, 0u)) >> 3; }
 
@@ -659,7 +980,7 @@ __device__ __forceinline__ void hll_word128(uint32_t w, int S, U128& sum, double
     }
 }
 
-template <int L>
+template <int L, bool ZM>
 __global__ void __launch_bounds__(256) hll_edges_kernel(const HllParams H) {
     const int lane = threadIdx.x & 31;
     const int sub = lane & (L - 1);
@@ -679,10 +1000,21 @@ __global__ void __launch_bounds__(256) hll_edges_kernel(const HllParams H) {
         const uint4* a4 = reinterpret_cast<const uint4*>(H.regs + su * (int64_t)m);
         const uint4* b4 = reinterpret_cast<const uint4*>(H.regs + sv * (int64_t)m);
         uint32_t zeros = 0;
+        if (ZM) {  // registers zero in both rows: AND of the two zero masks
+            const uint4* za = reinterpret_cast<const uint4*>(H.zm + su * (int64_t)H.zst);
+            const uint4* zb = reinterpret_cast<const uint4*>(H.zm + sv * (int64_t)H.zst);
 #pragma unroll 4
-        for (int i = sub; i < nvec; i += L) {
-            const uint4 a = __ldg(a4 + i), b = __ldg(b4 + i);
-            zeros += zero_bytes(a.x | b.x) + zero_bytes(a.y | b.y) + zero_bytes(a.z | b.z) + zero_bytes(a.w | b.w);
+            for (int i = sub; i < (H.zst >> 2); i += L) {
+                const uint4 a = __ldg(za + i), b = __ldg(zb + i);
+                zeros += __popc(a.x & b.x) + __popc(a.y & b.y) + __popc(a.z & b.z) + __popc(a.w & b.w);
+            }
+        } else {
+#pragma unroll 4
+            for (int i = sub; i < nvec; i += L) {
+                const uint4 a = __ldg(a4 + i), b = __ldg(b4 + i);
+                zeros += zero_bytes(a.x | b.x) + zero_bytes(a.y | b.y) + zero_bytes(a.z | b.z) +
+                         zero_bytes(a.w | b.w);
+            }
         }
         zeros = group_sum_u32<L>(zeros, gmask);
         double E;
@@ -748,7 +1080,13 @@ struct Tuning {
     int warps = 8;          // warps per CTA
     int pairs = 1;          // table-side / probe-side reorientation
     int sparse = 0;         // table load <= 1/4 where it fits
+    int hub = 256;          // pairs with d+(x) > hub go to the CTA-table kernel (0: off)
+    int hub_seg = 2048;     // hub pairs per CTA work unit
+    int hub_lg = 13;        // largest CTA table: 2^13 slots = 32 KB
+    int hub_unroll = 2;     // quads per lane in flight (2 or 4)
 };
+constexpr int HUB_MIN = 64;       // smallest hub threshold (bounds the segment count)
+constexpr int HUB_SEG_MIN = 256;  // smallest segment
 static Tuning g_tuning;
 
 // Optional phase timing: CUDA events recorded on the caller's stream around
@@ -800,11 +1138,15 @@ static int launch_count(const CountParams& P, bool details, cudaStream_t st) {
 }
 
 struct CountWs {
-    unsigned long long* ctr;  // work counters
-    int32_t* cnt;             // n_nodes + 1 (histogram)
+    unsigned long long* ctr;  // work counters: [0] [1] chunks, [2] hub segments made, [3] hub segments claimed
+    int32_t* cnt;             // n_nodes + 1 (histogram of small pairs)
     int32_t* off;             // n_nodes + 1 (scan, then scatter cursor)
+    int32_t* cnth;            // n_nodes + 1 (histogram of hub pairs)
+    int32_t* offh;            // n_nodes + 1
     int32_t* px;              // n_edges
-    int32_t* py;              // n_edges
+    int32_t* py;              // n_edges (small pairs, then the hub list)
+    HubSeg* segs;             // max_segs
+    int64_t max_segs;
     void* tmp;
     size_t tmp_bytes;
 };
@@ -818,8 +1160,13 @@ static bool carve_count(void* ws, size_t bytes, int64_t n_nodes, int64_t n_edges
     W.ctr = cv.take<unsigned long long>(4);
     W.cnt = cv.take<int32_t>(N);
     W.off = cv.take<int32_t>(N);
+    W.cnth = cv.take<int32_t>(N);
+    W.offh = cv.take<int32_t>(N);
     W.px = cv.take<int32_t>(E);
     W.py = cv.take<int32_t>(E);
+    // every hub x with pairs opens one segment, every HUB_SEG_MIN pairs at most one more
+    W.max_segs = (int64_t)(N < E ? N : E) + (int64_t)(E / HUB_SEG_MIN) + 1;
+    W.segs = cv.take<HubSeg>((size_t)W.max_segs);
     W.tmp_bytes = tb;
     W.tmp = cv.take<char>(tb);
     if (need) *need = cv.off;
@@ -827,15 +1174,23 @@ static bool carve_count(void* ws, size_t bytes, int64_t n_nodes, int64_t n_edges
 }
 
 // Hybrid calls also hold the HLL edge list (8 bytes per edge) after the
-// exact-count layout; exact-only calls use the prefix.
+// exact-count layout, then optionally the zero masks of the register rows
+// (zmask_words(p) words per row); exact-only calls use the prefix.
 struct HybridWs {
     int32_t* hll_u;
     int32_t* hll_v;
     unsigned long long* hll_n;
+    uint32_t* zm;  // null when the workspace was sized without masks
+    int zst;
 };
 
-static bool carve_count_hybrid(void* ws, size_t bytes, int64_t n_nodes, int64_t n_edges, CountWs& W, HybridWs& H,
-                               size_t* need) {
+static int zmask_words(int p) {
+    const int w = (1 << p) >> 5;
+    return w < 4 ? 4 : w;
+}
+
+static bool carve_count_hybrid(void* ws, size_t bytes, int64_t n_nodes, int64_t n_edges, int64_t zm_rows, int p,
+                               CountWs& W, HybridWs& H, size_t* need) {
     size_t base = 0;
     carve_count(nullptr, 0, n_nodes, n_edges, W, &base);
     const size_t E = (size_t)(n_edges > 0 ? n_edges : 1);
@@ -844,6 +1199,12 @@ static bool carve_count_hybrid(void* ws, size_t bytes, int64_t n_nodes, int64_t 
     H.hll_u = cv.take<int32_t>(E);
     H.hll_v = cv.take<int32_t>(E);
     H.hll_n = cv.take<unsigned long long>(1);
+    H.zm = nullptr;
+    H.zst = 0;
+    if (zm_rows > 0) {
+        H.zst = zmask_words(p);
+        H.zm = cv.take<uint32_t>((size_t)zm_rows * (size_t)H.zst);
+    }
     if (need) *need = cv.off;
     if (!cv.ok()) return false;
     if (!cv.dry) carve_count(b, base, n_nodes, n_edges, W, nullptr);
@@ -863,7 +1224,8 @@ static uint32_t lc_min_for(int p) {
 template <int L>
 static int launch_hll_edges_L(const HllParams& H, cudaStream_t st) {
     const int grid = sm_count() * 8;
-    hll_edges_kernel<L><<<grid, 256, 0, st>>>(H);
+    if (H.zm) hll_edges_kernel<L, true><<<grid, 256, 0, st>>>(H);
+    else hll_edges_kernel<L, false><<<grid, 256, 0, st>>>(H);
     TCHLL_CHECK_LAUNCH("hll_edges_kernel");
     return TCHLL_OK;
 }
@@ -880,8 +1242,19 @@ static int launch_hll_edges(const CountParams& P, const HybridWs& HW, cudaStream
     H.variant = P.variant;
     H.lc_min = lc_min_for(P.p);
     H.result = P.result;
-    const int nvec = (1 << P.p) >> 4;
-    switch (nvec >= 32 ? 32 : nvec) {
+    H.zm = HW.zm;
+    H.zst = HW.zst;
+    // Group width: one 16-byte load per lane per row for the first pass (the
+    // zero masks when present, else the registers); capped at a warp.
+    int width = HW.zm ? HW.zst >> 2 : (1 << P.p) >> 4;
+    if (HW.zm) {
+        const int64_t rows = P.slot ? P.n_rows : P.n_nodes;
+        const int64_t wgrid = (rows + 7) / 8;
+        const int grid = (int)(wgrid < 1 ? 1 : (wgrid > (int64_t)sm_count() * 16 ? (int64_t)sm_count() * 16 : wgrid));
+        zmask_kernel<<<grid, 256, 0, st>>>(P.regs, rows, P.slot ? nullptr : P.has, P.p, HW.zst, HW.zm);
+        TCHLL_CHECK_LAUNCH("zmask_kernel");
+    }
+    switch (width >= 32 ? 32 : width) {
         case 1: return launch_hll_edges_L<1>(H, st);
         case 2: return launch_hll_edges_L<2>(H, st);
         case 4: return launch_hll_edges_L<4>(H, st);
@@ -900,23 +1273,39 @@ static int grid_edges(int64_t n) {
 
 // Pair regrouping, part 1: histogram of table sides and its exclusive scan
 // (W.off[x] = first pair of x, W.off[n_nodes] = number of pairs).
+// With hub > 0 the histogram is split into small and hub pairs, both are
+// scanned, and the hub segments are listed (before the scatter moves offh).
 template <bool HYB>
-static int pairs_hist_scan(const CountParams& P, const CountWs& W, cudaStream_t st) {
+static int pairs_hist_scan(const CountParams& P, const CountWs& W, int hub, cudaStream_t st) {
     const int64_t N = P.n_nodes + 1;
     TCHLL_CUDA(cudaMemsetAsync(W.cnt, 0, sizeof(int32_t) * N, st));
     pair_hist_kernel<HYB><<<grid_edges(P.n_edges), 256, 0, st>>>(P, W.cnt);
     TCHLL_CHECK_LAUNCH("pair_hist_kernel");
+    if (hub > 0) {
+        hub_split_kernel<<<grid_edges(N), 256, 0, st>>>(P.row_ptr, P.n_nodes, hub, W.cnt, W.cnth);
+        TCHLL_CHECK_LAUNCH("hub_split_kernel");
+    }
     size_t tb = W.tmp_bytes;
     TCHLL_CUDA(cub::DeviceScan::ExclusiveSum(W.tmp, tb, W.cnt, W.off, (int)N, st));
     count_launch();
+    if (hub > 0) {
+        tb = W.tmp_bytes;
+        TCHLL_CUDA(cub::DeviceScan::ExclusiveSum(W.tmp, tb, W.cnth, W.offh, (int)N, st));
+        count_launch();
+        hub_segments_kernel<<<grid_edges(P.n_nodes), 256, 0, st>>>(W.cnth, W.offh, W.off + P.n_nodes, P.n_nodes,
+                                                                   g_tuning.hub_seg, W.segs, W.ctr + 2,
+                                                                   W.max_segs);
+        TCHLL_CHECK_LAUNCH("hub_segments_kernel");
+    }
     return TCHLL_OK;
 }
 
-// Part 2: scatter the pairs (advances W.off[x] for x < n_nodes only, so the
-// total in W.off[n_nodes] survives) and point Q at the pair list.
+// Part 2: scatter the pairs (advances W.off[x] / W.offh[x] for x < n_nodes
+// only, so the totals in [n_nodes] survive) and point Q at the small-pair list.
 template <bool HYB>
-static int pairs_scatter(const CountParams& P, const CountWs& W, CountParams& Q, cudaStream_t st) {
-    pair_scatter_kernel<HYB><<<grid_edges(P.n_edges), 256, 0, st>>>(P, W.off, W.px, W.py);
+static int pairs_scatter(const CountParams& P, const CountWs& W, int hub, CountParams& Q, cudaStream_t st) {
+    pair_scatter_kernel<HYB><<<grid_edges(P.n_edges), 256, 0, st>>>(P, W.off, W.offh, hub, W.off + P.n_nodes,
+                                                                   W.px, W.py);
     TCHLL_CHECK_LAUNCH("pair_scatter_kernel");
     Q = P;
     Q.edge_u = W.px;
@@ -925,20 +1314,67 @@ static int pairs_scatter(const CountParams& P, const CountWs& W, CountParams& Q,
     return TCHLL_OK;
 }
 
+// The hub pairs: one CTA per segment at a time, persistent grid.
+static int launch_hub(const CountParams& P, const CountWs& W, cudaStream_t st) {
+    HubParams H;
+    H.row_ptr = P.row_ptr;
+    H.col_idx = P.col_idx;
+    H.nnz = P.nnz;
+    H.hy = W.py;
+    H.segs = W.segs;
+    H.n_segs = W.ctr + 2;
+    H.max_segs = W.max_segs;
+    H.seg_ctr = W.ctr + 3;
+    H.hub_lg = g_tuning.hub_lg;
+    H.result = P.result;
+    auto kern = g_tuning.hub_unroll == 4 ? hub_count_kernel<4> : hub_count_kernel<2>;
+    const size_t smem = sizeof(int32_t) << g_tuning.hub_lg;
+    static size_t smem_set[2] = {0, 0};
+    size_t& done = smem_set[g_tuning.hub_unroll == 4 ? 1 : 0];
+    cudaError_t e;
+    if (smem > done) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(hub_count_kernel)");
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(hub_count_kernel carveout)");
+        done = smem;
+    }
+    int bps = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, 256, smem);
+    if (e != cudaSuccess) return cuda_status(e, "occupancy(hub_count_kernel)");
+    if (bps < 1) bps = 1;
+    kern<<<sm_count() * bps, 256, smem, st>>>(H);
+    TCHLL_CHECK_LAUNCH("hub_count_kernel");
+    return TCHLL_OK;
+}
+
+// Hub path in use: pairs on, and 16-byte aligned col_idx (quad loads).
+static int hub_threshold(const CountParams& P) {
+    return (g_tuning.hub > 0 && (uintptr_t)P.col_idx % 16 == 0) ? g_tuning.hub : 0;
+}
+
 // Build the grouped (x, y) pair list of the exact edges into Q.
 template <bool HYB>
-static int build_pairs(const CountParams& P, const CountWs& W, CountParams& Q, cudaStream_t st) {
-    int rc = pairs_hist_scan<HYB>(P, W, st);
+static int build_pairs(const CountParams& P, const CountWs& W, int hub, CountParams& Q, cudaStream_t st) {
+    int rc = pairs_hist_scan<HYB>(P, W, hub, st);
     if (rc) return rc;
-    return pairs_scatter<HYB>(P, W, Q, st);
+    return pairs_scatter<HYB>(P, W, hub, Q, st);
 }
 
 static int run_count(CountParams P, int mode, bool details, void* ws, size_t ws_bytes, cudaStream_t st) {
     CountWs W;
     HybridWs HW{};
     size_t need = 0;
-    const bool ok = (mode == MODE_EXACT) ? carve_count(ws, ws_bytes, P.n_nodes, P.n_edges, W, &need)
-                                         : carve_count_hybrid(ws, ws_bytes, P.n_nodes, P.n_edges, W, HW, &need);
+    bool ok;
+    if (mode == MODE_EXACT) {
+        ok = carve_count(ws, ws_bytes, P.n_nodes, P.n_edges, W, &need);
+    } else {
+        // With room for the zero masks the HLL pass reads them instead of
+        // the registers for the linear-counting test (same results).
+        const int64_t zm_rows = P.slot ? P.n_rows : P.n_nodes;
+        ok = zm_rows > 0 && carve_count_hybrid(ws, ws_bytes, P.n_nodes, P.n_edges, zm_rows, P.p, W, HW, &need);
+        if (!ok) ok = carve_count_hybrid(ws, ws_bytes, P.n_nodes, P.n_edges, 0, P.p, W, HW, &need);
+    }
     if (!ok || ws == nullptr) {
         set_error("workspace too small: need %zu bytes, have %zu", need, ws_bytes);
         return TCHLL_EWORKSPACE;
@@ -964,11 +1400,13 @@ static int run_count(CountParams P, int mode, bool details, void* ws, size_t ws_
         case MODE_EXACT:
             P.work = W.ctr;
             if (pairs) {
+                const int hub = hub_threshold(P);
                 phase_mark(0, st);
-                rc = build_pairs<false>(P, W, Q, st);
+                rc = build_pairs<false>(P, W, hub, Q, st);
                 if (rc) return rc;
                 phase_mark(1, st);
                 rc = launch_count<MODE_EXACT>(Q, false, st);
+                if (rc == TCHLL_OK && hub > 0) rc = launch_hub(P, W, st);
                 phase_mark(2, st);
                 g_phase.used[0] = g_phase.used[1] = true;
                 return rc;
@@ -997,15 +1435,20 @@ static int run_count(CountParams P, int mode, bool details, void* ws, size_t ws_
                 P.hll_v = HW.hll_v;
                 P.hll_n = HW.hll_n;
                 TCHLL_CUDA(cudaMemsetAsync(HW.hll_n, 0, sizeof(unsigned long long), st));
+                const int hub = hub_threshold(P);
                 phase_mark(0, st);
-                rc = pairs_hist_scan<true>(P, W, st);
+                rc = pairs_hist_scan<true>(P, W, hub, st);
                 if (rc) return rc;
-                rc = pairs_scatter<true>(P, W, Q, st);
+                rc = pairs_scatter<true>(P, W, hub, Q, st);
                 if (rc) return rc;
                 phase_mark(1, st);
                 Q.hll_u = nullptr;
                 rc = launch_count<MODE_EXACT>(Q, false, st);
                 if (rc) return rc;
+                if (hub > 0) {
+                    rc = launch_hub(P, W, st);
+                    if (rc) return rc;
+                }
                 phase_mark(2, st);
                 rc = launch_hll_edges(P, HW, st);
                 phase_mark(3, st);
@@ -1047,7 +1490,17 @@ TCHLL_EXPORT int tchll_count_workspace_bytes(int64_t n_nodes, int64_t n_edges, s
     TCHLL_ARG(bytes != nullptr && n_nodes >= 0 && n_edges >= 0, "bad arguments");
     CountWs W;
     HybridWs H;
-    carve_count_hybrid(nullptr, 0, n_nodes, n_edges, W, H, bytes);  // covers the exact-only layout too
+    carve_count_hybrid(nullptr, 0, n_nodes, n_edges, 0, 4, W, H, bytes);  // covers the exact-only layout too
+    return TCHLL_OK;
+}
+
+TCHLL_EXPORT int tchll_hybrid_workspace_bytes(int64_t n_nodes, int64_t n_edges, int64_t n_rows, int32_t p,
+                                              size_t* bytes) {
+    TCHLL_ARG(bytes != nullptr && n_nodes >= 0 && n_edges >= 0 && n_rows >= 0, "bad arguments");
+    TCHLL_ARG(p >= 4 && p <= 16, "p must be in [4, 16], got %d", p);
+    CountWs W;
+    HybridWs H;
+    carve_count_hybrid(nullptr, 0, n_nodes, n_edges, n_rows, p, W, H, bytes);
     return TCHLL_OK;
 }
 
@@ -1160,6 +1613,27 @@ TCHLL_EXPORT int tchll_set_count_table(int32_t sparse) {
     return TCHLL_OK;
 }
 
+TCHLL_EXPORT int tchll_set_count_hub(int32_t threshold, int32_t seg_pairs, int32_t table_log2, int32_t unroll) {
+    TCHLL_ARG(threshold == 0 || threshold >= HUB_MIN, "hub threshold must be 0 (off) or >= %d", HUB_MIN);
+    TCHLL_ARG(seg_pairs >= HUB_SEG_MIN && seg_pairs <= (1 << 20), "seg_pairs must be in [%d, 2^20]", HUB_SEG_MIN);
+    TCHLL_ARG(table_log2 >= 10 && table_log2 <= 15, "table_log2 must be in [10, 15]");
+    TCHLL_ARG(unroll == 2 || unroll == 4, "unroll must be 2 or 4");
+    g_tuning.hub = threshold;
+    g_tuning.hub_seg = seg_pairs;
+    g_tuning.hub_lg = table_log2;
+    g_tuning.hub_unroll = unroll;
+    return TCHLL_OK;
+}
+
+TCHLL_EXPORT int tchll_get_count_hub(int32_t* out4) {
+    TCHLL_ARG(out4 != nullptr, "null output");
+    out4[0] = g_tuning.hub;
+    out4[1] = g_tuning.hub_seg;
+    out4[2] = g_tuning.hub_lg;
+    out4[3] = g_tuning.hub_unroll;
+    return TCHLL_OK;
+}
+
 TCHLL_EXPORT int tchll_get_count_tuning(int32_t* out8) {
     TCHLL_ARG(out8 != nullptr, "out is null");
     out8[0] = g_tuning.chunk;
@@ -1238,8 +1712,8 @@ TCHLL_EXPORT int tchll_exact_count_noalloc(const int32_t* row_ptr, int64_t n_nod
     size_t need = 0;
     carve_count(nullptr, 0, n_nodes, n_edges, W, &need);
     if (need > (size_t)TCHLL_NOALLOC_SCRATCH_BYTES) {
-        set_error("graph too large for tchll_exact_count_noalloc: needs %zu bytes of scratch (8 per edge + 8 per "
-                  "vertex), the fixed limit is %u bytes; use tchll_exact_count with a workspace",
+        set_error("graph too large for tchll_exact_count_noalloc: needs %zu bytes of scratch (about 8 per edge + "
+                  "32 per vertex), the fixed limit is %u bytes; use tchll_exact_count with a workspace",
                   need, (unsigned)TCHLL_NOALLOC_SCRATCH_BYTES);
         return TCHLL_EINVAL;
     }
@@ -1413,13 +1887,13 @@ static int run_batch(CountParams P, bool hybrid, const int32_t* vbase, int64_t n
     phase_reset();
     P.work = B.cw.ctr;
     phase_mark(0, st);
-    if (hybrid) rc = pairs_hist_scan<true>(P, B.cw, st);
-    else rc = pairs_hist_scan<false>(P, B.cw, st);
+    if (hybrid) rc = pairs_hist_scan<true>(P, B.cw, 0, st);
+    else rc = pairs_hist_scan<false>(P, B.cw, 0, st);
     if (rc) return rc;
     rc = build_chunks(B.cw.off, vbase, n_graphs, P.n_nodes, B, st);  // pair ranges (before the scatter)
     if (rc) return rc;
-    if (hybrid) rc = pairs_scatter<true>(P, B.cw, Q, st);
-    else rc = pairs_scatter<false>(P, B.cw, Q, st);
+    if (hybrid) rc = pairs_scatter<true>(P, B.cw, 0, Q, st);
+    else rc = pairs_scatter<false>(P, B.cw, 0, Q, st);
     if (rc) return rc;
     phase_mark(1, st);
     Q.n_edges_dev = nullptr;

@@ -44,7 +44,7 @@ def cx_hybrid_count(g: core.DeviceCSR, regs: torch.Tensor, has: torch.Tensor, p:
     dev = g.device
     res = _lib.count_result_tensor(dev)
     nb = C.c_size_t(0)
-    check(load().tchll_count_workspace_bytes(g.n_nodes, g.n_edges, C.byref(nb)))
+    check(load().tchll_hybrid_workspace_bytes(g.n_nodes, g.n_edges, g.n_nodes, int(p), C.byref(nb)))
     ws = _lib.workspace.get(nb.value, dev)
     check(load().tchll_cx_hybrid_count(ptr(g.row_ptr), g.n_nodes, ptr(g.col_idx), g.n_edges, ptr(g.edge_u),
                                        ptr(g.edge_v), g.n_edges, ptr(g.degrees), ptr(regs), ptr(has), int(p),
