@@ -21,9 +21,13 @@
 //   * One persistent launch, work stealing: a warp claims CHUNK consecutive
 //     pairs with one atomicAdd and walks them 32 at a time; pairs sharing x
 //     form a group and reuse the warp's table (built once per group per chunk).
-//   * The table is bucketized cuckoo hashing (two hash functions, two-slot
-//     buckets, load <= 1/2): a lookup is two 8-byte shared loads and four
-//     compares, with no probe chains to diverge on.
+//   * The table keeps one 4-byte word per slot at load <= 1/8: a key sits in
+//     its home slot or, flagged there, on a second-hash walk, so a lookup is
+//     one 4-byte shared load with a rare walk (the warp seldom diverges).
+//   * Pairs whose x has a long list (d+(x) > hub threshold; 90% of the probes
+//     on R-MAT scale 22) are counted by a CTA-wide kernel: all warps of a CTA
+//     share one table of N+(x) of up to 32 KB, so long lists also get the
+//     low load factor.
 //   * The group's probe lists are flattened into one stream of 16-byte quads
 //     dealt to the 32 lanes by a warp scan, so short and long lists keep
 //     every lane busy.
@@ -94,53 +98,58 @@ struct CountParams {
     unsigned long long* hll_n;
 };
 
-// Bucketized cuckoo table: 2^lgb buckets of two int32 slots (one 8-byte
-// shared-memory word each); key x lives in bucket b1(x) or b2(x).  A lookup
-// is exactly two 8-byte loads and four compares -- no probe chains, so no
-// lane waits on another's collisions.
-struct Buckets {
-    uint32_t b1, b2;
-};
+// Hash table of one 4-byte word per slot (per-warp tables of the pair kernel
+// and the CTA tables of the hub kernel): bits 0-30 the key (0x7FFFFFFF =
+// empty; vertex ids stay below INT32_MAX) and bit 31 an overflow flag.  A
+// key lives in its home slot h1(k) when that was free at insertion; otherwise
+// it sets the flag on h1(k) and takes the first free slot of a linear walk
+// from h2(k).  A lookup reads the home slot: match -> hit; flag clear ->
+// miss; flag set (about load^2 of the slots) -> walk from h2(k) to the key or
+// a free slot.  At load <= 1/8 almost every lookup is ONE 4-byte shared load
+// and the warp rarely diverges.
+constexpr uint32_t OV_KEY = 0x7FFFFFFFu;   // key bits; this value marks an empty slot
+constexpr uint32_t OV_FLAG = 0x80000000u;  // some key of this home slot lives on its h2 walk
+constexpr uint32_t OV_NONE = 0x7FFFFFFEu;  // probe that matches no slot (vertex ids are below it)
 
-__device__ __forceinline__ Buckets tbl_buckets(int32_t x, int lgb) {
-    const uint64_t h = (uint64_t)(uint32_t)x * 0x9E3779B97F4A7C15ull;
-    Buckets r;
-    r.b1 = (uint32_t)(h >> (64 - lgb));
-    r.b2 = (uint32_t)(h >> (32 - lgb)) & ((1u << lgb) - 1u);
-    if (r.b2 == r.b1) r.b2 ^= 1u;
-    return r;
+__device__ __forceinline__ uint32_t ov_h1(int32_t x, int sh) { return ((uint32_t)x * 0x9E3779B1u) >> sh; }
+__device__ __forceinline__ uint32_t ov_h2(int32_t x, int sh) { return ((uint32_t)x * 0x85EBCA77u) >> sh; }
+
+// Claims slot h for key x if its key bits are empty (keeps the flag bit).
+// Returns 1 placed, 0 occupied by another key, 2 already holds x.
+__device__ __forceinline__ int ov_claim(uint32_t* T, uint32_t h, uint32_t x) {
+    uint32_t old = *(volatile uint32_t*)(T + h);
+    while ((old & OV_KEY) == OV_KEY) {
+        const uint32_t prev = atomicCAS(T + h, old, (old & OV_FLAG) | x);
+        if (prev == old) return 1;
+        old = prev;
+    }
+    return (old & OV_KEY) == x ? 2 : 0;
 }
 
-__device__ __forceinline__ uint32_t tbl_lookup(const int2* T, int32_t x, int lgb) {
-    const Buckets b = tbl_buckets(x, lgb);
-    const int2 p = T[b.b1];
-    const int2 q = T[b.b2];
-    return (uint32_t)((p.x == x) | (p.y == x) | (q.x == x) | (q.y == x));
-}
-
-// Inserts x (lane-parallel, shared-memory atomics; empty slots hold -1).
-// Returns false when the key could not be placed within the kick budget (the
-// caller then falls back to binary search for this table side).
-__device__ __forceinline__ bool tbl_insert(int32_t* T, int32_t x, int lgb) {
-    const Buckets xb = tbl_buckets(x, lgb);
-    if (atomicCAS(T + 2 * xb.b1, -1, x) == -1) return true;
-    if (atomicCAS(T + 2 * xb.b1 + 1, -1, x) == -1) return true;
-    if (atomicCAS(T + 2 * xb.b2, -1, x) == -1) return true;
-    if (atomicCAS(T + 2 * xb.b2 + 1, -1, x) == -1) return true;
-    // Both buckets full: cuckoo walk.  Take a slot of bucket b, move its
-    // resident to the resident's other bucket, and repeat there.  Slots never
-    // return to empty, so every evicted value is a real key.
-    int32_t cur = x;
-    uint32_t b = (x & 1) ? xb.b2 : xb.b1;
-    for (int kick = 0; kick < 128; ++kick) {
-        const int32_t victim = atomicExch(T + 2 * b + ((kick >> 1) & 1), cur);
-        cur = victim;
-        const Buckets vb = tbl_buckets(cur, lgb);
-        b = (b == vb.b1) ? vb.b2 : vb.b1;
-        if (atomicCAS(T + 2 * b, -1, cur) == -1) return true;
-        if (atomicCAS(T + 2 * b + 1, -1, cur) == -1) return true;
+// Inserts x; false only if the h2 walk finds no free slot (full table).
+__device__ __forceinline__ bool ov_insert(uint32_t* T, int32_t x, int sh, uint32_t mask) {
+    const uint32_t h = ov_h1(x, sh);
+    if (ov_claim(T, h, (uint32_t)x)) return true;
+    atomicOr(T + h, OV_FLAG);
+    uint32_t g = ov_h2(x, sh);
+    for (uint32_t i = 0; i <= mask; ++i) {
+        if (ov_claim(T, g, (uint32_t)x)) return true;
+        g = (g + 1u) & mask;
     }
     return false;
+}
+
+// The h2 walk of a lookup whose home slot was flagged: 1 at x, 0 at a free
+// slot; at most mask + 1 steps.
+__device__ __forceinline__ uint32_t ov_walk(const uint32_t* T, int32_t x, int sh, uint32_t mask) {
+    uint32_t g = ov_h2(x, sh);
+    for (uint32_t i = 0; i <= mask; ++i) {
+        const uint32_t k = T[g] & OV_KEY;
+        if (k == (uint32_t)x) return 1u;
+        if (k == OV_KEY) return 0u;
+        g = (g + 1u) & mask;
+    }
+    return 0u;
 }
 
 __device__ __forceinline__ int ceil_log2_i(int x) { return x <= 1 ? 0 : 32 - __clz(x - 1); }
@@ -332,13 +341,13 @@ __device__ __forceinline__ void publish(tchll_count_result* R, uint64_t acc, U12
 }
 
 template <int MODE, bool VEC, bool DETAILS>
-__global__ void __launch_bounds__(256, 1) count_kernel(const CountParams P) {
+__global__ void __launch_bounds__(256, 3) count_kernel(const CountParams P) {
     extern __shared__ __align__(16) int32_t smem[];
     const int lane = threadIdx.x & 31;
     const int wid = threadIdx.x >> 5;
     const int cap_lg = P.slots_log2;
     const int cap_keys = 1 << (cap_lg - 1);  // load <= 1/2 in 2^cap_lg slots
-    int32_t* table = smem + ((size_t)wid << cap_lg);
+    uint32_t* table = reinterpret_cast<uint32_t*>(smem) + ((size_t)wid << cap_lg);
 
     const int32_t* __restrict__ col_idx = P.col_idx;
     const int64_t n_edges = P.n_edges_dev ? (int64_t)*P.n_edges_dev : P.n_edges;
@@ -348,7 +357,7 @@ __global__ void __launch_bounds__(256, 1) count_kernel(const CountParams P) {
     int64_t n_approx = 0, n_exact = 0, n_fallback = 0, n_clamped = 0;
     uint32_t status = 0;
     int cur_u = -1;
-    int cur_lg = 4;  // log2 buckets of the current table
+    int cur_lg = 5;  // log2 slots of the current table
     const int m = 1 << P.p;
 
     while (true) {
@@ -432,21 +441,22 @@ __global__ void __launch_bounds__(256, 1) count_kernel(const CountParams P) {
                     continue;
                 }
                 if (ucur != cur_u) {
-                    // (re)build the warp's table for N+(ucur): 2^lgb buckets,
-                    // load gdu / 2^(lgb+1) <= 1/4 when the capacity allows,
+                    // (re)build the warp's table for N+(ucur): 2^lgs slots,
+                    // load <= 1/8 (1/16 sparse) when the capacity allows,
                     // <= 1/2 always
-                    int lgb = ceil_log2_i(gdu) + (P.sparse ? 1 : 0);
-                    lgb = lgb < 4 ? 4 : (lgb > cap_lg - 1 ? cap_lg - 1 : lgb);
-                    const int nslots = 2 << lgb;
+                    int lgs = ceil_log2_i(gdu) + (P.sparse ? 4 : 3);
+                    lgs = lgs < 5 ? 5 : (lgs > cap_lg ? cap_lg : lgs);
+                    const int nslots = 1 << lgs;
                     __syncwarp();
                     for (int i = lane; i < (nslots >> 2); i += 32)
-                        reinterpret_cast<int4*>(table)[i] = make_int4(-1, -1, -1, -1);
+                        reinterpret_cast<uint4*>(table)[i] = make_uint4(OV_KEY, OV_KEY, OV_KEY, OV_KEY);
                     __syncwarp();
                     bool ok = true;
-                    for (int i = lane; i < gdu; i += 32) ok &= tbl_insert(table, __ldg(col_idx + gus + i), lgb);
+                    for (int i = lane; i < gdu; i += 32)
+                        ok &= ov_insert(table, __ldg(col_idx + gus + i), 32 - lgs, (uint32_t)nslots - 1u);
                     __syncwarp();
                     if (!__all_sync(FULL, ok)) {
-                        // cuckoo placement failed: binary search for this group
+                        // no free slot (cannot happen at load <= 1/2): binary search for this group
                         cur_u = -1;
                         unsigned g = grp;
                         while (g) {
@@ -465,9 +475,10 @@ __global__ void __launch_bounds__(256, 1) count_kernel(const CountParams P) {
                         continue;
                     }
                     cur_u = ucur;
-                    cur_lg = lgb;
+                    cur_lg = lgs;
                 }
-                const int2* T2 = reinterpret_cast<const int2*>(table);
+                const int sh = 32 - cur_lg;
+                const uint32_t tmask = (1u << cur_lg) - 1u;
                 // flatten the group's probe lists into quads
                 int q0, nq;
                 if (VEC) {
@@ -547,21 +558,47 @@ __global__ void __launch_bounds__(256, 1) count_kernel(const CountParams P) {
                             }
                         }
                     }
+                    // home slots of every key first (branch-free; elements
+                    // outside the pair's list probe as OV_NONE), then the
+                    // rare walks of flagged homes
+                    constexpr int KPQ = VEC ? 4 : 1;  // keys per quad
+                    uint32_t key[KPQ * UNR];
 #pragma unroll
                     for (int i = 0; i < UNR; ++i) {
-                        if (qd[i] < 0) continue;
-                        uint32_t c = 0;
+                        // mapped quads have lo <= KPQ - 1 and hi >= 1; unmapped: lo = hi = 0
+                        key[KPQ * i + 0] = (lo[i] <= 0 && hi[i] > 0) ? (uint32_t)val[i].x : OV_NONE;
                         if (VEC) {
-                            c += (0 >= lo[i] && 0 < hi[i]) ? tbl_lookup(T2, val[i].x, cur_lg) : 0u;
-                            c += (1 >= lo[i] && 1 < hi[i]) ? tbl_lookup(T2, val[i].y, cur_lg) : 0u;
-                            c += (2 >= lo[i] && 2 < hi[i]) ? tbl_lookup(T2, val[i].z, cur_lg) : 0u;
-                            c += (3 >= lo[i] && 3 < hi[i]) ? tbl_lookup(T2, val[i].w, cur_lg) : 0u;
-                        } else {
-                            c = tbl_lookup(T2, val[i].x, cur_lg);
+                            key[KPQ * i + 1] = (lo[i] <= 1 && hi[i] > 1) ? (uint32_t)val[i].y : OV_NONE;
+                            key[KPQ * i + 2] = (lo[i] <= 2 && hi[i] > 2) ? (uint32_t)val[i].z : OV_NONE;
+                            key[KPQ * i + 3] = (lo[i] <= 3 && hi[i] > 3) ? (uint32_t)val[i].w : OV_NONE;
                         }
-                        acc += c;
-                        if (DETAILS && c)
-                            atomicAdd((unsigned long long*)(P.pe_support + my_e[i]), (unsigned long long)c);
+                    }
+                    const uint32_t* T = table;
+                    uint32_t cq[UNR], pend = 0;
+#pragma unroll
+                    for (int i = 0; i < UNR; ++i) {
+                        cq[i] = 0;
+#pragma unroll
+                        for (int j = 0; j < KPQ; ++j) {
+                            const int t = KPQ * i + j;
+                            const uint32_t d = T[ov_h1((int32_t)key[t], sh)] ^ key[t];
+                            cq[i] += (d << 1) == 0u;
+                            pend |= (d > OV_FLAG ? 1u : 0u) << t;
+                        }
+                    }
+                    if (pend) {
+#pragma unroll
+                        for (int i = 0; i < UNR; ++i)
+#pragma unroll
+                            for (int j = 0; j < KPQ; ++j)
+                                if ((pend >> (KPQ * i + j)) & 1u)
+                                    cq[i] += ov_walk(T, (int32_t)key[KPQ * i + j], sh, tmask);
+                    }
+#pragma unroll
+                    for (int i = 0; i < UNR; ++i) {
+                        acc += cq[i];
+                        if (DETAILS && cq[i])
+                            atomicAdd((unsigned long long*)(P.pe_support + my_e[i]), (unsigned long long)cq[i]);
                     }
                 }
             }
@@ -618,16 +655,8 @@ __global__ void __launch_bounds__(256, 1) count_kernel(const CountParams P) {
 // sum of min(d+u, d+v) has d+(x) > 256).  They are counted one x at a time
 // by a whole CTA: the CTA builds ONE table of N+(x) in shared memory at load
 // <= 1/8 (up to 2^hub_lg slots) and its warps stream the probe lists of x's
-// pairs through it.
-//
-// Table: one 4-byte word per slot, bits 0-30 the key (0x7FFFFFFF = empty;
-// vertex ids stay below INT32_MAX) and bit 31 an overflow flag.  A key lives
-// in its home slot h1(k) when that was free at insertion; otherwise it sets
-// the flag on h1(k) and takes the first free slot of a linear walk from
-// h2(k).  A lookup reads the home slot: match -> hit; flag clear -> miss; flag
-// set (about load^2 of the slots) -> walk from h2(k) to the key or a free
-// slot.  So almost every lookup is ONE 4-byte shared load and the warp rarely
-// diverges, against two 8-byte loads for the per-warp cuckoo table.
+// pairs through it (a per-warp table of 8 KB would hold N+(x) only at load
+// up to 1/2, where the overflow walks of the one-load table grow).
 struct HubSeg {
     int64_t start;  // first pair in the hub list
     int32_t x;
@@ -646,51 +675,6 @@ struct HubParams {
     int hub_lg;  // log2 of the largest table (slots)
     tchll_count_result* result;
 };
-
-constexpr uint32_t OV_KEY = 0x7FFFFFFFu;   // key bits; this value marks an empty slot
-constexpr uint32_t OV_FLAG = 0x80000000u;  // some key of this home slot lives on its h2 walk
-constexpr uint32_t OV_NONE = 0x7FFFFFFEu;  // probe that matches no slot (vertex ids are below it)
-
-__device__ __forceinline__ uint32_t ov_h1(int32_t x, int sh) { return ((uint32_t)x * 0x9E3779B1u) >> sh; }
-__device__ __forceinline__ uint32_t ov_h2(int32_t x, int sh) { return ((uint32_t)x * 0x85EBCA77u) >> sh; }
-
-// Claims slot h for key x if its key bits are empty (keeps the flag bit).
-// Returns 1 placed, 0 occupied by another key, 2 already holds x.
-__device__ __forceinline__ int ov_claim(uint32_t* T, uint32_t h, uint32_t x) {
-    uint32_t old = *(volatile uint32_t*)(T + h);
-    while ((old & OV_KEY) == OV_KEY) {
-        const uint32_t prev = atomicCAS(T + h, old, (old & OV_FLAG) | x);
-        if (prev == old) return 1;
-        old = prev;
-    }
-    return (old & OV_KEY) == x ? 2 : 0;
-}
-
-// Inserts x; false only if the h2 walk finds no free slot (full table).
-__device__ __forceinline__ bool ov_insert(uint32_t* T, int32_t x, int sh, uint32_t mask) {
-    const uint32_t h = ov_h1(x, sh);
-    if (ov_claim(T, h, (uint32_t)x)) return true;
-    atomicOr(T + h, OV_FLAG);
-    uint32_t g = ov_h2(x, sh);
-    for (uint32_t i = 0; i <= mask; ++i) {
-        if (ov_claim(T, g, (uint32_t)x)) return true;
-        g = (g + 1u) & mask;
-    }
-    return false;
-}
-
-// The h2 walk of a lookup whose home slot was flagged: 1 at x, 0 at a free
-// slot; at most mask + 1 steps.
-__device__ __forceinline__ uint32_t ov_walk(const uint32_t* T, int32_t x, int sh, uint32_t mask) {
-    uint32_t g = ov_h2(x, sh);
-    for (uint32_t i = 0; i <= mask; ++i) {
-        const uint32_t k = T[g] & OV_KEY;
-        if (k == (uint32_t)x) return 1u;
-        if (k == OV_KEY) return 0u;
-        g = (g + 1u) & mask;
-    }
-    return 0u;
-}
 
 template <int UNR>
 __global__ void __launch_bounds__(256, 4) hub_count_kernel(const HubParams H) {
