@@ -176,10 +176,12 @@ int tchll_exact_count_noalloc(const int32_t* row_ptr, int64_t n_nodes, const int
  * When enabled, the counting entry points record CUDA events on the
  * caller's stream around their phases; tchll_phase_times then waits for the
  * last call's events and writes milliseconds: ms3[0] pair regrouping,
- * ms3[1] exact-count kernel, ms3[2] HLL kernel (-1 for a phase the call did
- * not run). */
+ * ms3[1] exact-count kernels (pair kernel and hub kernel), ms3[2] HLL kernel
+ * (-1 for a phase the call did not run).  tchll_phase_hub_ms writes the hub
+ * kernel's share of ms3[1] (-1 when it did not run). */
 int tchll_set_phase_timing(int32_t enable);
 int tchll_phase_times(float* ms3 /* host */);
+int tchll_phase_hub_ms(float* ms /* host */);
 
 /* ------------------------------------------------------------ sketches --- */
 /*

@@ -151,11 +151,11 @@ def test_c5_requests_shape():
     assert estimate_bytes(reqs[0]) > 40 * reqs[0].raw_edges()
 
 
-def _serve_mix(dev, n=60, rate=400.0, budget=120e9, scale_range=(8, 12), repeat=0.3):
+def _serve_mix(dev, n=60, rate=400.0, budget=120e9, scale_range=(8, 12), repeat=0.3, big_edges=1 << 20):
     from triangle_counting_hll_b200 import serve as S
     reqs = S.c5_requests(n, rate, seed=5, scale_range=scale_range, ef_range=(4, 16), repeat_frac=repeat,
                          p=10, theta=16)
-    srv = S.Server(dev, budget_bytes=budget, max_batch=32)
+    srv = S.Server(dev, budget_bytes=budget, max_batch=32, big_edges=big_edges)
     return reqs, srv, srv.serve(reqs)
 
 
@@ -164,8 +164,11 @@ def test_server_results_same_alone_and_in_the_mix(tchll):
     import torch
     from triangle_counting_hll_b200 import serve as S
     dev = torch.device("cuda", 0)
-    reqs, srv, got = _serve_mix(dev)
+    # graphs of >= 2^14 raw edges take the single-graph path, smaller ones are
+    # batched (a burst of arrivals, so that ticks hold several small graphs)
+    reqs, srv, got = _serve_mix(dev, rate=1e5, big_edges=1 << 14)
     assert len(got) == len(reqs) and all(c.error is None for c in got)
+    assert srv.stats["single_launches"] > 0 and srv.stats["batched_launches"] > 0
     assert srv.stats["ticks"] < len(reqs)          # queries were batched
     assert max(srv.stats["batch_sizes"]) > 1
     assert srv.stats["cache_hits"] > 0             # repeat queries reused resident graphs

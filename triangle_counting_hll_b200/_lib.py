@@ -74,6 +74,7 @@ SIGNATURES = {
     "tchll_exact_count_noalloc": (C.c_int, [_P, _I64, _P, _I64, _P, _P, _I64, _P, _P]),
     "tchll_set_phase_timing": (C.c_int, [_I32]),
     "tchll_phase_times": (C.c_int, [_P]),
+    "tchll_phase_hub_ms": (C.c_int, [_P]),
     "tchll_sketch_workspace_bytes": (C.c_int, [_I64, C.POINTER(_SZ)]),
     "tchll_build_sketches_dense": (C.c_int, [_P, _I64, _P, _I64, _I64, _I32, _P, _P, _P]),
     "tchll_sketch_slots": (C.c_int, [_P, _I64, _I64, _P, _P, _P, _SZ, _P]),
@@ -203,15 +204,18 @@ def stream_handle(device=None) -> int:
 
 
 class Workspace:
-    """Grow-only device scratch buffer owned by the caller side (the library
-    never allocates).  One per device and purpose."""
+    """Grow-only device scratch buffers owned by the caller side (the library
+    never allocates), one per (device, current stream): a buffer is only ever
+    used by work on the stream it was allocated on, so the caching allocator
+    never hands its memory to another stream while a kernel still reads it."""
 
     def __init__(self):
         self._buf = {}
 
     def get(self, nbytes: int, device) -> torch.Tensor:
         dev = torch.device(device)
-        key = dev.index if dev.index is not None else torch.cuda.current_device()
+        idx = dev.index if dev.index is not None else torch.cuda.current_device()
+        key = (idx, torch.cuda.current_stream(idx).cuda_stream)
         b = self._buf.get(key)
         if b is None or b.numel() < nbytes:
             b = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=dev)

@@ -289,7 +289,11 @@ def phase_times() -> dict:
     out = (C.c_float * 3)()
     check(load().tchll_phase_times(C.cast(out, C.c_void_p)))
     names = ("pairs", "count", "hll")
-    return {n: (float(v) if v >= 0 else None) for n, v in zip(names, out)}
+    res = {n: (float(v) if v >= 0 else None) for n, v in zip(names, out)}
+    hub = C.c_float(-1.0)
+    check(load().tchll_phase_hub_ms(C.byref(hub)))
+    res["hub"] = float(hub.value) if hub.value >= 0 else None  # part of "count"
+    return res
 
 
 # ----------------------------------------------------------- sketches (a4)

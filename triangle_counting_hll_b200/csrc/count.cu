@@ -658,9 +658,10 @@ __global__ void __launch_bounds__(256, 3) count_kernel(const CountParams P) {
 // pairs through it (a per-warp table of 8 KB would hold N+(x) only at load
 // up to 1/2, where the overflow walks of the one-load table grow).
 struct HubSeg {
-    int64_t start;  // first pair in the hub list
+    int32_t start;  // first pair in the hub list (pair lists hold < 2^31 entries)
     int32_t x;
     int32_t len;
+    int32_t graph;  // batched counts: the graph of x (its result block); else 0
 };
 
 struct HubParams {
@@ -672,7 +673,8 @@ struct HubParams {
     const unsigned long long* n_segs;
     int64_t max_segs;
     unsigned long long* seg_ctr;
-    int hub_lg;  // log2 of the largest table (slots)
+    int hub_lg;    // log2 of the largest table (slots)
+    bool batched;  // publish per segment into result[segment graph]
     tchll_count_result* result;
 };
 
@@ -827,8 +829,16 @@ __global__ void __launch_bounds__(256, 4) hub_count_kernel(const HubParams H) {
                 acc += c;
             }
         }
+        if (H.batched) {  // this segment's totals belong to its graph
+            acc = warp_sum_u64(acc);
+            if (lane == 0 && acc) atomicAdd((unsigned long long*)&H.result[sg.graph].exact, (unsigned long long)acc);
+            if (tid == 0) atomicAdd((unsigned long long*)&H.result[sg.graph].n_exact, (unsigned long long)sg.len);
+            acc = 0;
+            n_pairs = 0;
+        }
         __syncthreads();  // every warp is done with this table
     }
+    if (H.batched) return;
     acc = warp_sum_u64(acc);
     n_pairs = warp_sum_i64(n_pairs);
     if (lane == 0) {
@@ -839,22 +849,35 @@ __global__ void __launch_bounds__(256, 4) hub_count_kernel(const HubParams H) {
 
 // Hub segments: x's hub pairs [offh[x], offh[x] + cnth[x]) (shifted by the
 // small-pair total *n_small) cut into pieces of at most seg pairs.
+// Batched counts (vbase != null) record the graph of x, found by binary
+// search in the ascending vertex offsets vbase[0..n_graphs].
 __global__ void hub_segments_kernel(const int32_t* __restrict__ cnth, const int32_t* __restrict__ offh,
                                     const int32_t* __restrict__ n_small, int64_t n_nodes, int seg, HubSeg* segs,
-                                    unsigned long long* n_segs, int64_t max_segs) {
-    const int64_t base_pairs = (int64_t)*n_small;
+                                    unsigned long long* n_segs, int64_t max_segs, const int32_t* __restrict__ vbase,
+                                    int64_t n_graphs) {
+    const int32_t base_pairs = *n_small;
     for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < n_nodes;
          x += (int64_t)gridDim.x * blockDim.x) {
         const int32_t c = __ldg(cnth + x);
         if (c <= 0) continue;
+        int32_t g = 0;
+        if (vbase) {  // last g with vbase[g] <= x
+            int64_t lo = 0, hi = n_graphs - 1;
+            while (lo < hi) {
+                const int64_t mid = (lo + hi + 1) >> 1;
+                if (__ldg(vbase + mid) <= x) lo = mid; else hi = mid - 1;
+            }
+            g = (int32_t)lo;
+        }
         const int k = (c + seg - 1) / seg;
         const unsigned long long b = atomicAdd(n_segs, (unsigned long long)k);
         for (int j = 0; j < k; ++j) {
             if ((int64_t)(b + j) >= max_segs) break;  // cannot happen: sized for the worst case
             HubSeg s;
-            s.start = base_pairs + __ldg(offh + x) + (int64_t)j * seg;
+            s.start = base_pairs + __ldg(offh + x) + j * seg;
             s.x = (int32_t)x;
             s.len = min(seg, c - j * seg);
+            s.graph = g;
             segs[b + j] = s;
         }
     }
@@ -1079,7 +1102,9 @@ struct PhaseTimer {
     bool on = false;
     bool made = false;
     cudaEvent_t ev[4];
+    cudaEvent_t hub_ev[2];  // around the hub kernel, inside phase 1
     bool used[3] = {false, false, false};
+    bool hub_used = false;
 };
 static PhaseTimer g_phase;
 
@@ -1088,6 +1113,7 @@ static void phase_mark(int i, cudaStream_t st) {
 }
 static void phase_reset() {
     for (int i = 0; i < 3; ++i) g_phase.used[i] = false;
+    g_phase.hub_used = false;
 }
 
 template <int MODE, bool VEC, bool DETAILS>
@@ -1260,7 +1286,8 @@ static int grid_edges(int64_t n) {
 // With hub > 0 the histogram is split into small and hub pairs, both are
 // scanned, and the hub segments are listed (before the scatter moves offh).
 template <bool HYB>
-static int pairs_hist_scan(const CountParams& P, const CountWs& W, int hub, cudaStream_t st) {
+static int pairs_hist_scan(const CountParams& P, const CountWs& W, int hub, cudaStream_t st,
+                           const int32_t* vbase = nullptr, int64_t n_graphs = 0) {
     const int64_t N = P.n_nodes + 1;
     TCHLL_CUDA(cudaMemsetAsync(W.cnt, 0, sizeof(int32_t) * N, st));
     pair_hist_kernel<HYB><<<grid_edges(P.n_edges), 256, 0, st>>>(P, W.cnt);
@@ -1278,7 +1305,7 @@ static int pairs_hist_scan(const CountParams& P, const CountWs& W, int hub, cuda
         count_launch();
         hub_segments_kernel<<<grid_edges(P.n_nodes), 256, 0, st>>>(W.cnth, W.offh, W.off + P.n_nodes, P.n_nodes,
                                                                    g_tuning.hub_seg, W.segs, W.ctr + 2,
-                                                                   W.max_segs);
+                                                                   W.max_segs, vbase, n_graphs);
         TCHLL_CHECK_LAUNCH("hub_segments_kernel");
     }
     return TCHLL_OK;
@@ -1299,8 +1326,9 @@ static int pairs_scatter(const CountParams& P, const CountWs& W, int hub, CountP
 }
 
 // The hub pairs: one CTA per segment at a time, persistent grid.
-static int launch_hub(const CountParams& P, const CountWs& W, cudaStream_t st) {
+static int launch_hub(const CountParams& P, const CountWs& W, cudaStream_t st, bool batched = false) {
     HubParams H;
+    H.batched = batched;
     H.row_ptr = P.row_ptr;
     H.col_idx = P.col_idx;
     H.nnz = P.nnz;
@@ -1327,8 +1355,13 @@ static int launch_hub(const CountParams& P, const CountWs& W, cudaStream_t st) {
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, 256, smem);
     if (e != cudaSuccess) return cuda_status(e, "occupancy(hub_count_kernel)");
     if (bps < 1) bps = 1;
+    if (g_phase.on && g_phase.made) cudaEventRecord(g_phase.hub_ev[0], st);
     kern<<<sm_count() * bps, 256, smem, st>>>(H);
     TCHLL_CHECK_LAUNCH("hub_count_kernel");
+    if (g_phase.on && g_phase.made) {
+        cudaEventRecord(g_phase.hub_ev[1], st);
+        g_phase.hub_used = true;
+    }
     return TCHLL_OK;
 }
 
@@ -1634,6 +1667,7 @@ TCHLL_EXPORT int tchll_get_count_tuning(int32_t* out8) {
 TCHLL_EXPORT int tchll_set_phase_timing(int32_t enable) {
     if (enable && !g_phase.made) {
         for (int i = 0; i < 4; ++i) TCHLL_CUDA(cudaEventCreate(&g_phase.ev[i]));
+        for (int i = 0; i < 2; ++i) TCHLL_CUDA(cudaEventCreate(&g_phase.hub_ev[i]));
         g_phase.made = true;
     }
     g_phase.on = enable != 0;
@@ -1650,6 +1684,15 @@ TCHLL_EXPORT int tchll_phase_times(float* ms3) {
         TCHLL_CUDA(cudaEventSynchronize(g_phase.ev[i + 1]));
         TCHLL_CUDA(cudaEventElapsedTime(&ms3[i], g_phase.ev[i], g_phase.ev[i + 1]));
     }
+    return TCHLL_OK;
+}
+
+TCHLL_EXPORT int tchll_phase_hub_ms(float* ms) {
+    TCHLL_ARG(ms != nullptr, "out is null");
+    *ms = -1.0f;
+    if (!g_phase.on || !g_phase.made || !g_phase.hub_used) return TCHLL_OK;
+    TCHLL_CUDA(cudaEventSynchronize(g_phase.hub_ev[1]));
+    TCHLL_CUDA(cudaEventElapsedTime(ms, g_phase.hub_ev[0], g_phase.hub_ev[1]));
     return TCHLL_OK;
 }
 
@@ -1871,18 +1914,25 @@ static int run_batch(CountParams P, bool hybrid, const int32_t* vbase, int64_t n
     phase_reset();
     P.work = B.cw.ctr;
     phase_mark(0, st);
-    if (hybrid) rc = pairs_hist_scan<true>(P, B.cw, 0, st);
-    else rc = pairs_hist_scan<false>(P, B.cw, 0, st);
+    // pairs with a long table side go to the hub kernel, which publishes
+    // per segment into the graph of x
+    const int hub = hub_threshold(P);
+    if (hybrid) rc = pairs_hist_scan<true>(P, B.cw, hub, st, vbase, n_graphs);
+    else rc = pairs_hist_scan<false>(P, B.cw, hub, st, vbase, n_graphs);
     if (rc) return rc;
     rc = build_chunks(B.cw.off, vbase, n_graphs, P.n_nodes, B, st);  // pair ranges (before the scatter)
     if (rc) return rc;
-    if (hybrid) rc = pairs_scatter<true>(P, B.cw, 0, Q, st);
-    else rc = pairs_scatter<false>(P, B.cw, 0, Q, st);
+    if (hybrid) rc = pairs_scatter<true>(P, B.cw, hub, Q, st);
+    else rc = pairs_scatter<false>(P, B.cw, hub, Q, st);
     if (rc) return rc;
     phase_mark(1, st);
     Q.n_edges_dev = nullptr;
     rc = launch_count<MODE_EXACT>(Q, false, st);
     if (rc) return rc;
+    if (hub > 0) {
+        rc = launch_hub(P, B.cw, st, true);
+        if (rc) return rc;
+    }
     phase_mark(2, st);
     g_phase.used[0] = g_phase.used[1] = true;
     if (!hybrid) return TCHLL_OK;

@@ -10,12 +10,14 @@ The reference answers one query per call, synchronously (src/gpu_hybrid.py:
   resident; least-recently-used resident graphs are evicted to make room, and
   a request that could never fit is completed with an error;
 * graphs stay resident after their query, so repeat queries skip the build;
-* every tick, the newly admitted graphs are built together (one concatenated
-  device CSR build, split into per-graph residents) on a build stream while
-  the previous tick's counts run on a count stream, so arrivals overlap with
-  work already on the device; then all admitted queries of the tick are
-  folded into one batched count launch per mode (exact, hybrid), whose
-  per-graph results are bit-identical to answering each query alone;
+* every tick, the newly admitted graphs are built on a build stream while
+  earlier counts run on a count stream, so arrivals overlap with work
+  already on the device: small graphs are counted together (one batched
+  count launch per mode, exact and hybrid, over their concatenated CSRs),
+  large graphs (at least ``big_edges`` raw edges, which fill the GPU on their
+  own) one at a time, each count launched as soon as its graph is built;
+  finished counts are answered as the host sees them.
+  Per-graph results are bit-identical to answering each query alone;
 * latency is completion time minus arrival time; the report gives p50 / p99
   and graphs/s next to the same requests served one at a time.
 """
@@ -98,8 +100,13 @@ def estimate_bytes(req: Request) -> int:
     m = req.raw_edges()
     b = 40 * m + 16 * (1 << req.scale)
     if req.mode == "hybrid":
-        b += (2 * m // max(req.theta, 1) + 1) << req.p
+        b += sketch_bytes(req)
     return b
+
+
+def sketch_bytes(req: Request) -> int:
+    """At most 2m/theta rows of 2^p registers plus the per-vertex slots."""
+    return ((2 * req.raw_edges() // max(req.theta, 1) + 1) << req.p) + 8 * (1 << req.scale)
 
 
 @dataclass
@@ -107,24 +114,8 @@ class Resident:
     csr: core.DeviceCSR
     nbytes: int
     last_use: float = 0.0
-
-
-def split_batch(bt: B.GraphBatch) -> List[core.DeviceCSR]:
-    """Per-graph CSRs (each with its own 0-based ids) out of a concatenated
-    batch build."""
-    g = bt.csr
-    vb = bt.vbase.cpu().numpy().astype(np.int64)
-    eb_all = g.row_ptr[bt.vbase.long()].cpu().numpy().astype(np.int64)  # edge range of each graph
-    out = []
-    for i in range(bt.n_graphs):
-        a, b = int(vb[i]), int(vb[i + 1])
-        ea, eb = int(eb_all[i]), int(eb_all[i + 1])
-        row_ptr = (g.row_ptr[a:b + 1] - ea).contiguous()
-        col = (g.col_idx[ea:eb] - a).contiguous()
-        eu = (g.edge_u[ea:eb] - a).contiguous()
-        ids = (g.node_ids[a:b] - int(bt.id_base[i])).contiguous()
-        out.append(core.DeviceCSR(row_ptr, col, g.degrees[a:b].contiguous(), ids, eu, col.clone()))
-    return out
+    # compact sketches per (p, theta), built with the graph for hybrid queries
+    sketches: Dict[Tuple[int, int], Tuple[torch.Tensor, torch.Tensor]] = field(default_factory=dict)
 
 
 def concat_csrs(csrs: Sequence[core.DeviceCSR], device) -> B.GraphBatch:
@@ -150,19 +141,36 @@ def concat_csrs(csrs: Sequence[core.DeviceCSR], device) -> B.GraphBatch:
     return B.GraphBatch(csr, vbase, voff)
 
 
+_STREAMS: Dict[int, Tuple[torch.cuda.Stream, torch.cuda.Stream]] = {}
+
+
+def _server_streams(dev: torch.device) -> Tuple[torch.cuda.Stream, torch.cuda.Stream]:
+    """The (build, count) stream pair of a device, shared by every Server on
+    it: torch's caching allocator keeps a block pool per stream, so fresh
+    streams per server would pay device allocations again."""
+    idx = dev.index if dev.index is not None else torch.cuda.current_device()
+    if idx not in _STREAMS:
+        _STREAMS[idx] = (torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev))
+    return _STREAMS[idx]
+
+
 class Server:
     def __init__(self, device=None, budget_bytes: float = 120e9, max_batch: int = 256,
-                 max_batch_edges: float = 4e8):
+                 max_batch_edges: float = 4e8, big_edges: int = 1 << 20):
         self.dev = core._device(device)
+        self.big_edges = int(big_edges)
         self.budget = int(budget_bytes)
         self.max_batch = max_batch
         self.max_batch_edges = int(max_batch_edges)
         self.resident: "collections.OrderedDict[Tuple, Resident]" = collections.OrderedDict()
         self.resident_bytes = 0
-        self.build_stream = torch.cuda.Stream(device=self.dev)
-        self.count_stream = torch.cuda.Stream(device=self.dev)
-        self.stats = {"ticks": 0, "built": 0, "cache_hits": 0, "evicted": 0, "rejected": 0, "batch_sizes": []}
-        self.busy: set = set()  # keys whose graphs the in-flight launch reads
+        self.build_stream, self.count_stream = _server_streams(self.dev)
+        self.stats = {"ticks": 0, "built": 0, "cache_hits": 0, "evicted": 0, "rejected": 0, "batch_sizes": [],
+                      "single_launches": 0, "batched_launches": 0}
+        self.busy: set = set()  # keys whose graphs the in-flight launches read
+        self.pending: list = []  # launched, unanswered: (mode, requests, results, event, buffers)
+        self._done: List[Completion] = []
+        self._t0 = 0.0
 
     # ----------------------------------------------------------- memory
     def _evict_for(self, need: int, pinned: set) -> bool:
@@ -184,7 +192,12 @@ class Server:
         edges = 0
         while queue and len(taken) < self.max_batch:
             r = queue[0]
-            need = 0 if r.key in self.resident else estimate_bytes(r)
+            if r.key in self.resident:  # sketches of a resident graph may still be missing
+                res = self.resident[r.key]
+                need = sketch_bytes(r) if (r.mode == "hybrid" and res.csr.n_edges >= self.big_edges
+                                           and (r.p, r.theta) not in res.sketches) else 0
+            else:
+                need = estimate_bytes(r)
             if need > self.budget:
                 queue.popleft()
                 self.stats["rejected"] += 1
@@ -203,8 +216,8 @@ class Server:
         return taken
 
     def _build(self, reqs: List[Request]) -> None:
-        """Build the graphs of reqs that are not resident (one concatenated
-        device build on the build stream), and make them resident."""
+        """Build the graphs of reqs that are not resident (device CSR builds
+        on the build stream), and make them resident."""
         todo: Dict[Tuple, Request] = {}
         for r in reqs:
             if r.key in self.resident:
@@ -213,18 +226,34 @@ class Server:
                 todo.setdefault(r.key, r)
         if not todo:
             return
+        built = []
         with torch.cuda.stream(self.build_stream):
-            items = []
-            for r in todo.values():
-                u, v = generate_edges(r, self.dev)
-                items.append((u, v, 1 << r.scale))
-            bt = B.GraphBatch.from_edge_lists(items, device=self.dev)
-            parts = split_batch(bt)
-        for (key, r), csr in zip(todo.items(), parts):
+            for kr in todo.items():
+                u, v = generate_edges(kr[1], self.dev)
+                built.append((kr, core.csr_from_edges(u, v, device=self.dev)))
+                del u, v
+        for (key, r), csr in built:
             nb = csr.nbytes()
             self.resident[key] = Resident(csr, nb)
             self.resident_bytes += nb
             self.stats["built"] += 1
+
+    def _sketch(self, reqs: List[Request]) -> None:
+        """Compact sketches of the large graphs of hybrid queries, on the build
+        stream (their row count is read back here, not in the launch stage,
+        so the count stream is never waited on while launching)."""
+        with torch.cuda.stream(self.build_stream):
+            for r in reqs:
+                res = self.resident[r.key]
+                if r.mode != "hybrid" or res.csr.n_edges < self.big_edges or (r.p, r.theta) in res.sketches:
+                    continue
+                g = res.csr
+                slot, n_rows = core.sketch_slots(g.row_ptr, r.theta)
+                rows = core.build_sketches_compact_tensors(g.row_ptr, g.col_idx, slot, n_rows, r.p)
+                res.sketches[(r.p, r.theta)] = (rows, slot)
+                nb = rows.numel() + slot.numel() * slot.element_size()
+                res.nbytes += nb
+                self.resident_bytes += nb
 
     def _launch(self, reqs: List[Request]):
         """Fold the tick's queries into one batched launch per mode on the
@@ -240,85 +269,122 @@ class Server:
                 for c in csrs:  # built on the build stream, read here
                     for t in (c.row_ptr, c.col_idx, c.degrees, c.node_ids, c.edge_u, c.edge_v):
                         t.record_stream(self.count_stream)
-                res = torch.empty(len(group) * _lib.RESULT_BYTES, dtype=torch.uint8, device=self.dev)
                 r0 = group[0]  # one (p, theta, gamma) per launch; the workload uses one setting
-                if len(group) == 1:
-                    # a lone query runs the single-graph path directly (same
-                    # kernels and integer totals, no concatenation)
-                    bt = None
-                    g = csrs[0]
+                # large graphs, and a lone query, run the single-graph path
+                # (same kernels and integer totals, no concatenation)
+                lone = [i for i, g in enumerate(csrs) if len(group) == 1 or g.n_edges >= self.big_edges]
+                lone_set = set(lone)
+                rest = [i for i in range(len(group)) if i not in lone_set]
+                keep = []
+                for i in lone:
+                    g = csrs[i]
+                    res = torch.empty(_lib.RESULT_BYTES, dtype=torch.uint8, device=self.dev)
                     if mode == "exact":
                         core.exact_count_tensors(g.row_ptr, g.col_idx, g.edge_u, g.edge_v, result=res)
                     else:
-                        slot, n_rows = core.sketch_slots(g.row_ptr, r0.theta)
-                        rows = core.build_sketches_compact_tensors(g.row_ptr, g.col_idx, slot, n_rows, r0.p)
+                        sk = self.resident[group[i].key].sketches.get((r0.p, r0.theta))
+                        if sk is None:  # a lone query on a small graph
+                            slot, n_rows = core.sketch_slots(g.row_ptr, r0.theta)
+                            rows = core.build_sketches_compact_tensors(g.row_ptr, g.col_idx, slot, n_rows, r0.p)
+                        else:
+                            rows, slot = sk
+                            rows.record_stream(self.count_stream)
+                            slot.record_stream(self.count_stream)
                         core.hybrid_count_compact_tensors(g.row_ptr, g.col_idx, g.edge_u, g.edge_v, g.degrees,
                                                           rows, slot, r0.p, r0.gamma, split_kernels=True,
                                                           result=res)
-                        bt = (rows, slot)
-                else:
-                    bt = concat_csrs(csrs, self.dev)
+                        keep.append((rows, slot))
+                    ev = torch.cuda.Event()
+                    ev.record(self.count_stream)
+                    pending.append((mode, [group[i]], res, ev, keep))
+                    self.stats["single_launches"] += 1
+                if rest:
+                    sub = [group[i] for i in rest]
+                    res = torch.empty(len(sub) * _lib.RESULT_BYTES, dtype=torch.uint8, device=self.dev)
+                    bt = concat_csrs([csrs[i] for i in rest], self.dev)
                     if mode == "exact":
                         bt.exact_launch(res)
                     else:
                         rows, slot = bt.sketches(r0.theta, r0.p)
                         bt.hybrid_launch(res, rows, slot, r0.p, r0.gamma)
-                ev = torch.cuda.Event()
-                ev.record(self.count_stream)
-                pending.append((mode, group, res, ev, bt))
+                    ev = torch.cuda.Event()
+                    ev.record(self.count_stream)
+                    pending.append((mode, sub, res, ev, bt))
+                    self.stats["batched_launches"] += 1
         for r in reqs:
             if r.key in self.resident:
                 self.resident.move_to_end(r.key)
-        self.busy = {r.key for r in reqs}
         return pending
 
-    def _finish(self, pending, done: List[Completion], t0: float) -> None:
-        for mode, group, res, ev, bt in pending:
-            ev.synchronize()
-            now = time.perf_counter() - t0
-            try:
-                if mode == "exact":
-                    vals = B.exact_from_results(res, len(group))
-                    for r, v in zip(group, vals):
-                        done.append(Completion(r.rid, mode, int(v), latency=now - r.arrival))
-                else:
-                    tot, st = B.hybrid_from_results(res, len(group))
-                    for i, r in enumerate(group):
-                        done.append(Completion(r.rid, mode, float(tot[i]), {k: int(st[k][i]) for k in st},
-                                               latency=now - r.arrival))
-            except ValueError as exc:  # malformed input: fail this group's queries only
-                for r in group:
-                    done.append(Completion(r.rid, mode, None, latency=now - r.arrival, error=str(exc)))
+    def _complete(self, item, done: List[Completion], t0: float) -> None:
+        mode, group, res, ev, _ = item
+        now = time.perf_counter() - t0
+        try:
+            if mode == "exact":
+                vals = B.exact_from_results(res, len(group))
+                for r, v in zip(group, vals):
+                    done.append(Completion(r.rid, mode, int(v), latency=now - r.arrival))
+            else:
+                tot, st = B.hybrid_from_results(res, len(group))
+                for i, r in enumerate(group):
+                    done.append(Completion(r.rid, mode, float(tot[i]), {k: int(st[k][i]) for k in st},
+                                           latency=now - r.arrival))
+        except ValueError as exc:  # malformed input: fail this group's queries only
+            for r in group:
+                done.append(Completion(r.rid, mode, None, latency=now - r.arrival, error=str(exc)))
+
+    def _reap(self, block: bool = False) -> None:
+        """Answer every launched query whose count has finished (the oldest
+        one first, waiting for it when block is set); a query's latency ends
+        when the host sees its result."""
+        keep = []
+        for k, item in enumerate(self.pending):
+            if block and k == 0:
+                item[3].synchronize()
+            if not keep and item[3].query():
+                self._complete(item, self._done, self._t0)
+            else:
+                keep.append(item)  # the count stream finishes launches in order
+        self.pending = keep
+        self.busy = {r.key for it in self.pending for r in it[1]}
 
     # -------------------------------------------------------------- loop
     def serve(self, requests: Sequence[Request]) -> List[Completion]:
+        """Serve requests in real time (arrival = seconds after the call);
+        returns one Completion per request, ordered by request id.  Launches
+        of several ticks may be in flight on the count stream at once."""
         reqs = sorted(requests, key=lambda r: r.arrival)
         queue: "collections.deque[Request]" = collections.deque()
-        done: List[Completion] = []
-        t0 = time.perf_counter()
+        self._done: List[Completion] = []
+        self._t0 = t0 = time.perf_counter()
+        self.pending = []
         i = 0
-        inflight = None
-        while len(done) < len(reqs):
+        while len(self._done) < len(reqs):
             now = time.perf_counter() - t0
             while i < len(reqs) and reqs[i].arrival <= now:
                 queue.append(reqs[i])
                 i += 1
-            nxt = self._admit(queue, done, now) if queue else []
-            if nxt:
-                self._build(nxt)              # overlaps with the in-flight counts
-            if inflight is not None:
-                self._finish(inflight, done, t0)
-                inflight = None
-                self.busy = set()
+            self._reap()
+            nxt = self._admit(queue, self._done, now) if queue else []
             if nxt:
                 self.stats["ticks"] += 1
                 self.stats["batch_sizes"].append(len(nxt))
-                inflight = self._launch(nxt)
+                # small graphs: one batched build and launch; large graphs:
+                # each built and launched in turn, so its count runs while
+                # the host builds the next one
+                small = [r for r in nxt if r.raw_edges() < self.big_edges]
+                stages = ([small] if small else []) + [[r] for r in nxt if r.raw_edges() >= self.big_edges]
+                for part in stages:
+                    self._build(part)         # overlaps with the in-flight counts
+                    self._sketch(part)
+                    self.pending += self._launch(part)
+                    self.busy = {r.key for it in self.pending for r in it[1]}
+                    self._reap()
+            elif self.pending:
+                self._reap(block=True)
             elif not queue and i < len(reqs):
                 time.sleep(max(0.0, min(reqs[i].arrival - (time.perf_counter() - t0), 0.002)))
-        if inflight is not None:
-            self._finish(inflight, done, t0)
-        return sorted(done, key=lambda c: c.rid)
+        return sorted(self._done, key=lambda c: c.rid)
 
 
 def serve_sequential(requests: Sequence[Request], device=None) -> List[Completion]:
@@ -372,6 +438,14 @@ def bench_entry(dev, quick: bool = True) -> Dict:
     n = 300 if quick else 20000
     out: Dict = {"requests_per_rate": n, "workload": "R-MAT scale U[12,20], ef U[8,32], 50/50 exact / hybrid "
                  "(p=12, theta=gamma=128), Poisson arrivals, 120 GB admission budget"}
+    # warm both paths (allocator pools of the server streams and the default
+    # stream, lazy kernel loading) on requests outside the timed sets
+    warm = [Request(i, 0.0, 20, 32, 777 + i, m) for i, m in enumerate(("exact", "hybrid", "exact", "hybrid"))]
+    warm += c5_requests(40, 1e6, seed=12345)
+    for _ in range(2):
+        Server(dev, budget_bytes=120e9).serve(warm)
+        serve_sequential(warm, dev)
+    torch.cuda.synchronize(dev)
     for rate in (50.0, 200.0, 1000.0):
         reqs = c5_requests(n, rate, seed=int(rate))
         srv = Server(dev, budget_bytes=120e9)
