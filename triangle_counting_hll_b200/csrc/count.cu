@@ -1254,9 +1254,16 @@ static int launch_hll_edges(const CountParams& P, const HybridWs& HW, cudaStream
     H.result = P.result;
     H.zm = HW.zm;
     H.zst = HW.zst;
-    // Group width: one 16-byte load per lane per row for the first pass (the
-    // zero masks when present, else the registers); capped at a warp.
-    int width = HW.zm ? HW.zst >> 2 : (1 << P.p) >> 4;
+    // Group width (lanes per edge, at most a warp).  Without zero masks: one
+    // 16-byte register load per lane per row.  With them, for p >= 11 the
+    // linear-counting shortcut settles almost every edge from the masks
+    // alone, a pass bound by the latency of its dependent loads: four mask
+    // loads per lane per row, several edges per warp in flight.  For p = 9, 10
+    // most edges also need the register pass, which runs better on wider
+    // groups: one mask load per lane.  For p <= 8 one lane per edge.
+    // (Measured on R-MAT scale 22, theta = 256.)
+    int width = (1 << P.p) >> 4;
+    if (HW.zm) width = P.p >= 11 ? HW.zst >> 4 : (P.p >= 9 ? HW.zst >> 2 : 1);
     if (HW.zm) {
         const int64_t rows = P.slot ? P.n_rows : P.n_nodes;
         const int64_t wgrid = (rows + 7) / 8;
