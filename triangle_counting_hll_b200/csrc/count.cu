@@ -987,7 +987,7 @@ __device__ __forceinline__ void hll_word128(uint32_t w, int S, U128& sum, double
     }
 }
 
-template <int L, bool ZM>
+template <int L, bool ZM, bool CACHE>
 __global__ void __launch_bounds__(256) hll_edges_kernel(const HllParams H) {
     const int lane = threadIdx.x & 31;
     const int sub = lane & (L - 1);
@@ -1000,7 +1000,19 @@ __global__ void __launch_bounds__(256) hll_edges_kernel(const HllParams H) {
     const int S = 65 - H.p;
     U128 hacc;
     int64_t n_approx = 0, n_clamped = 0;
-    for (int64_t e = gid; e < n; e += ngroups) {
+    // CACHE: each group takes a contiguous run of the edge list.  The routing
+    // pass appends edges in CSR order, so consecutive HLL edges mostly share u
+    // and the group keeps u's zero mask in registers across them (up to four
+    // 16-byte words per lane).  Otherwise the groups stride over the list.
+    const int64_t per = CACHE ? (n + ngroups - 1) / ngroups : 1;
+    const int64_t e_lo = CACHE ? gid * per : gid;
+    const int64_t e_hi = CACHE ? min(n, e_lo + per) : n;
+    const int64_t e_step = CACHE ? 1 : ngroups;
+    const int nq = H.zst >> 2;
+    const bool cache_a = CACHE && ZM && nq <= 4 * L;
+    int64_t cached = -1;
+    uint4 ca[4];
+    for (int64_t e = e_lo; e < e_hi; e += e_step) {
         const int32_t u = __ldg(H.hu + e), v = __ldg(H.hv + e);
         const int64_t su = H.slot ? __ldg(H.slot + u) : (int64_t)u;
         const int64_t sv = H.slot ? __ldg(H.slot + v) : (int64_t)v;
@@ -1010,10 +1022,30 @@ __global__ void __launch_bounds__(256) hll_edges_kernel(const HllParams H) {
         if (ZM) {  // registers zero in both rows: AND of the two zero masks
             const uint4* za = reinterpret_cast<const uint4*>(H.zm + su * (int64_t)H.zst);
             const uint4* zb = reinterpret_cast<const uint4*>(H.zm + sv * (int64_t)H.zst);
+            if (cache_a) {
+                if (su != cached) {  // group-uniform
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const int i = sub + k * L;
+                        ca[k] = i < nq ? __ldg(za + i) : make_uint4(0u, 0u, 0u, 0u);
+                    }
+                    cached = su;
+                }
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int i = sub + k * L;
+                    if (i < nq) {
+                        const uint4 b = __ldg(zb + i);
+                        zeros += __popc(ca[k].x & b.x) + __popc(ca[k].y & b.y) + __popc(ca[k].z & b.z) +
+                                 __popc(ca[k].w & b.w);
+                    }
+                }
+            } else {
 #pragma unroll 4
-            for (int i = sub; i < (H.zst >> 2); i += L) {
-                const uint4 a = __ldg(za + i), b = __ldg(zb + i);
-                zeros += __popc(a.x & b.x) + __popc(a.y & b.y) + __popc(a.z & b.z) + __popc(a.w & b.w);
+                for (int i = sub; i < nq; i += L) {
+                    const uint4 a = __ldg(za + i), b = __ldg(zb + i);
+                    zeros += __popc(a.x & b.x) + __popc(a.y & b.y) + __popc(a.z & b.z) + __popc(a.w & b.w);
+                }
             }
         } else {
 #pragma unroll 4
@@ -1234,8 +1266,9 @@ static uint32_t lc_min_for(int p) {
 template <int L>
 static int launch_hll_edges_L(const HllParams& H, cudaStream_t st) {
     const int grid = sm_count() * 8;
-    if (H.zm) hll_edges_kernel<L, true><<<grid, 256, 0, st>>>(H);
-    else hll_edges_kernel<L, false><<<grid, 256, 0, st>>>(H);
+    if (H.zm && H.p >= 11) hll_edges_kernel<L, true, true><<<grid, 256, 0, st>>>(H);
+    else if (H.zm) hll_edges_kernel<L, true, false><<<grid, 256, 0, st>>>(H);
+    else hll_edges_kernel<L, false, false><<<grid, 256, 0, st>>>(H);
     TCHLL_CHECK_LAUNCH("hll_edges_kernel");
     return TCHLL_OK;
 }
