@@ -340,7 +340,11 @@ def run_hybrid_line(args, g, dev, rank, world, barrier, max_over_ranks):
     hll = torch.minimum(du, dv) >= theta
     n_hll = int(hll.sum().item())
     exact_bytes = 16 * (g.n_edges - n_hll) + 4 * int(torch.where(hll, 0, du + dv).sum().item())
+    hub_thr = core.get_count_tuning()["hub"]
+    hub = (~hll) & (torch.maximum(du, dv) > hub_thr) if hub_thr > 0 else torch.zeros_like(hll)
+    hub_bytes = 16 * int(hub.sum().item()) + 4 * int(torch.where(hub, du + dv, 0).sum().item())
     hll_bytes = n_hll * (16 + 2 * (1 << p))
+    del du, dv, hll, hub
     res = _lib.count_result_tensor(dev)
     ex_res, _ = core.exact_count_tensors(g.row_ptr, g.col_idx, g.edge_u, g.edge_v)
     exact = core.exact_from_result(ex_res)
@@ -398,12 +402,13 @@ def run_hybrid_line(args, g, dev, rank, world, barrier, max_over_ranks):
     del host
 
     peaks = load_peaks()
-    if avg["hll"] > avg["count"]:
-        kname, kms, kbytes = "hll_edges_kernel", avg["hll"], hll_bytes
-    else:
-        kname, kms, kbytes = "count_kernel<exact pairs>", avg["count"], exact_bytes
+    # the dominant kernel of the three: HLL pass, hub pairs, other exact pairs
+    hub_ms = avg.get("hub") or 0.0
+    cands = [("hll_edges_kernel", avg["hll"], hll_bytes), ("hub_count_kernel", hub_ms, hub_bytes),
+             ("count_kernel", avg["count"] - hub_ms, exact_bytes - hub_bytes)]
+    kname, kms, kbytes = max(cands, key=lambda c: c[1])
     achieved = kbytes / (kms / 1e3) / 1e9
-    traffic = load_traffic(f"rmat{args.scale}_ef16_hybrid_p{p}_{kname.split('<')[0]}")
+    traffic = load_traffic(f"rmat{args.scale}_ef16_hybrid_p{p}_theta{theta}:{kname}")
     line = {
         "metric": METRIC, "value": world * g.n_edges / (ms_step / 1e3), "unit": "edges/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
@@ -421,7 +426,9 @@ def run_hybrid_line(args, g, dev, rank, world, barrier, max_over_ranks):
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peaks["hbm_gbs"],
                      "peak_source": peaks["source"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
                      "kernel_ms": kms, "algorithmic_bytes": kbytes,
-                     "traffic": traffic["bytes_per_launch"] if traffic else None},
+                     "traffic": traffic["bytes_per_launch"] if traffic else None,
+                     "traffic_source": traffic["source"] if traffic else None,
+                     "kernels": {c[0]: {"ms": c[1], "algorithmic_bytes": c[2]} for c in cands}},
         "gpu_launches": launches,
         "clocks": clk,
     }

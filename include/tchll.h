@@ -160,8 +160,10 @@ int tchll_get_count_hub(int32_t* out4 /* host */);
  * result as tchll_exact_count without per-edge output, but the scratch comes
  * from a fixed array of TCHLL_NOALLOC_SCRATCH_BYTES inside the library that
  * every GPU loading the library reserves until the process exits; graphs
- * needing more scratch (8 bytes per edge + 8 per vertex, so roughly
- * n_nodes + n_edges <= 4 million) are rejected with TCHLL_EINVAL.  The first
+ * needing more scratch (about 8 bytes per edge + 32 per vertex: the pair
+ * lists, four per-vertex histograms / offsets and the work-unit list, so for
+ * example 3 M edges on 200 K vertices fit) are rejected with TCHLL_EINVAL.
+ * The first
  * call on a device looks up the array's device address; make that first call
  * before any stream capture.  All calls share the one array: calls that
  * overlap on the GPU (different streams or devices sharing a context) race;
