@@ -679,7 +679,7 @@ struct HubParams {
 };
 
 template <int UNR>
-__global__ void __launch_bounds__(256, 4) hub_count_kernel(const HubParams H) {
+__global__ void __launch_bounds__(256, 5) hub_count_kernel(const HubParams H) {
     extern __shared__ __align__(16) uint32_t tbl[];
     __shared__ HubSeg s_seg;
     __shared__ int s_round;
@@ -821,10 +821,14 @@ __global__ void __launch_bounds__(256, 4) hub_count_kernel(const HubParams H) {
                     c += (d << 1) == 0u;                       // key bits equal
                     pend |= (d > OV_FLAG ? 1u : 0u) << t;      // flagged home, other key
                 }
-                if (pend) {
+                // each lane walks its own flagged homes (usually none or one)
+                while (pend) {
+                    const int t = __ffs(pend) - 1;
+                    pend &= pend - 1u;
+                    uint32_t k = key[0];
 #pragma unroll
-                    for (int t = 0; t < 4 * UNR; ++t)
-                        if ((pend >> t) & 1u) c += ov_walk(tbl, (int32_t)key[t], sh, mask);
+                    for (int j = 1; j < 4 * UNR; ++j) k = (t == j) ? key[j] : k;
+                    c += ov_walk(tbl, (int32_t)k, sh, mask);
                 }
                 acc += c;
             }
