@@ -73,6 +73,38 @@ def test_batched_exact_bit_exact_vs_one_at_a_time(tchll, oracle):
 
 
 @pytest.mark.gpu
+def test_batched_hub_segments_go_to_their_graph(tchll, oracle):
+    """Graphs with long forward lists (cliques of 300 and 400 vertices, and
+    an R-MAT graph) between small ones: the hub kernel's segments publish
+    into the right graph's result (exact and hybrid), equal to one graph at a
+    time and to the oracle."""
+    import torch
+    from triangle_counting_hll_b200 import batch as B
+    from triangle_counting_hll_b200 import core
+    dev = torch.device("cuda", 0)
+    items = _small_batch(dev, 12)
+    for k, pos in ((300, 2), (400, 9)):
+        iu, iv = np.triu_indices(k, 1)
+        items.insert(pos, (torch.from_numpy((iu * 7).astype(np.int32)).to(dev),
+                           torch.from_numpy((iv * 7).astype(np.int32)).to(dev), 7 * k))
+    u, v = core.gen_rmat(14, 32, 0.57, 0.19, 0.19, seed=9, device=dev)
+    items.insert(5, (u, v, 1 << 14))
+    bt = B.GraphBatch.from_edge_lists(items, device=dev)
+    csrs = [core.csr_from_edges(a, b, device=dev) for a, b, _ in items]
+    assert max(int(c.degrees.max()) for c in csrs if c.n_nodes) > core.get_count_tuning()["hub"]
+    got = bt.exact_counts()
+    assert np.array_equal(got, B.plain_exact_counts(csrs))
+    assert got[2] == 300 * 299 * 298 // 6 and got[10] == 400 * 399 * 398 // 6
+    og = oracle.csr_build(u.cpu().numpy(), v.cpu().numpy())
+    assert got[5] == oracle.exact_count(og["row_ptr"], og["col_idx"], og["edge_u"], og["edge_v"])
+    tot, st = bt.hybrid_counts(64, 64, 10)
+    rtot, rst = B.plain_hybrid_counts(csrs, B.plain_sketches(csrs, 64, 10), 64, 10)
+    assert np.array_equal(tot, rtot)
+    for k in rst:
+        assert np.array_equal(st[k], rst[k]), k
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("theta,p", [(8, 10), (16, 8), (4, 12)])
 def test_batched_hybrid_bit_exact_vs_one_at_a_time(tchll, theta, p):
     import torch
