@@ -669,6 +669,7 @@ struct HubParams {
     const int32_t* col_idx;
     int64_t nnz;
     const int32_t* hy;  // y of each hub pair, grouped by x
+    const int32_t* pcol;  // padded lists (pad_rows_kernel) or null
     const HubSeg* segs;
     const unsigned long long* n_segs;
     int64_t max_segs;
@@ -678,7 +679,31 @@ struct HubParams {
     tchll_count_result* result;
 };
 
-template <int UNR>
+// Padded probe lists: row y's list starts at element pad_start(y), a multiple
+// of 4, and is followed by OV_NONE up to the next multiple of 4, so every
+// 16-byte quad holds only the list's keys or OV_NONE and no probe needs a
+// mask.  pad_start(y) = roundup4(row_ptr[y]) + 8 y leaves room for the
+// padding of every row before y (at most 3 per row) without a scan.
+__device__ __forceinline__ int64_t pad_start(int32_t rs, int32_t y) {
+    return (((int64_t)rs + 3) & ~(int64_t)3) + 8 * (int64_t)y;
+}
+
+__global__ void pad_rows_kernel(const int32_t* __restrict__ row_ptr, int64_t n_nodes,
+                                const int32_t* __restrict__ col, int32_t* __restrict__ pcol) {
+    const int sub = threadIdx.x & 7;  // 8 lanes per row
+    const int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 3;
+    const int64_t ng = ((int64_t)gridDim.x * blockDim.x) >> 3;
+    for (int64_t y = g; y < n_nodes; y += ng) {
+        const int32_t rs = __ldg(row_ptr + y);
+        const int32_t d = __ldg(row_ptr + y + 1) - rs;
+        if (d <= 0) continue;
+        const int64_t ps = pad_start(rs, (int32_t)y);
+        const int32_t len = (d + 3) & ~3;
+        for (int32_t i = sub; i < len; i += 8) pcol[ps + i] = i < d ? __ldg(col + rs + i) : (int32_t)OV_NONE;
+    }
+}
+
+template <int UNR, bool PAD>
 __global__ void __launch_bounds__(256, 5) hub_count_kernel(const HubParams H) {
     extern __shared__ __align__(16) uint32_t tbl[];
     __shared__ HubSeg s_seg;
@@ -728,17 +753,24 @@ __global__ void __launch_bounds__(256, 5) hub_count_kernel(const HubParams H) {
             r = __shfl_sync(FULL, r, 0);
             if (r >= sg.len) break;
             const int np = min(32, sg.len - r);
-            int32_t vs = 0, ve = 0;
+            int32_t rs = 0, re = 0, vs = 0, ve = 0;
             if (lane < np) {
                 const int32_t y = __ldg(H.hy + sg.start + r + lane);
-                vs = __ldg(H.row_ptr + y);
-                ve = __ldg(H.row_ptr + y + 1);
+                rs = __ldg(H.row_ptr + y);
+                re = __ldg(H.row_ptr + y + 1);
+                if (PAD) {
+                    vs = (int32_t)pad_start(rs, y);
+                    ve = vs + ((re - rs + 3) & ~3);
+                } else {
+                    vs = rs;
+                    ve = re;
+                }
             }
             if (!table) {  // x's list too long for the table: binary search per pair
                 for (int j = 0; j < np; ++j) {
-                    const int32_t jvs = __shfl_sync(FULL, vs, j);
-                    const int32_t jve = __shfl_sync(FULL, ve, j);
-                    acc += warp_bsearch_count(col + xs, xl, col + jvs, jve - jvs, lane);
+                    const int32_t jrs = __shfl_sync(FULL, rs, j);
+                    const int32_t jre = __shfl_sync(FULL, re, j);
+                    acc += warp_bsearch_count(col + xs, xl, col + jrs, jre - jrs, lane);
                 }
                 continue;
             }
@@ -780,55 +812,72 @@ __global__ void __launch_bounds__(256, 5) hub_count_kernel(const HubParams H) {
                         const int32_t my_ve = __shfl_sync(FULL, c_ve, j);
                         if (Ti + lane < W) {
                             qd[i] = my_qb + Ti + lane;
-                            lo[i] = my_vs - qd[i] * 4;  // valid elements of the quad: [lo, hi)
-                            hi[i] = my_ve - qd[i] * 4;
+                            if (!PAD) {
+                                lo[i] = my_vs - qd[i] * 4;  // valid elements of the quad: [lo, hi)
+                                hi[i] = my_ve - qd[i] * 4;
+                            }
                         }
                     }
                 }
-                int4 val[UNR];
-#pragma unroll
-                for (int i = 0; i < UNR; ++i) {
-                    val[i] = make_int4(-1, -1, -1, -1);
-                    if (qd[i] >= 0) {
-                        const int64_t base = (int64_t)qd[i] * 4;
-                        if (base + 3 < H.nnz) {
-                            val[i] = __ldg(reinterpret_cast<const int4*>(col) + qd[i]);
-                        } else {
-                            val[i].x = base + 0 < H.nnz ? __ldg(col + base + 0) : -1;
-                            val[i].y = base + 1 < H.nnz ? __ldg(col + base + 1) : -1;
-                            val[i].z = base + 2 < H.nnz ? __ldg(col + base + 2) : -1;
-                            val[i].w = base + 3 < H.nnz ? __ldg(col + base + 3) : -1;
-                        }
-                    }
-                }
-                // Home slots of all 4 * UNR keys, branch-free: elements
-                // outside the pair's list (quad edges, idle lanes) probe as
-                // OV_NONE, which matches no slot.  Then the rare walks of
-                // flagged homes.
+                // Keys of all 4 * UNR quad elements.  Elements outside the
+                // pair's list (quad edges, idle lanes) probe as OV_NONE,
+                // which matches no slot; padded lists need no masking.
                 uint32_t key[4 * UNR];
 #pragma unroll
                 for (int i = 0; i < UNR; ++i) {
-                    // lo <= 3 and hi >= 1 for every mapped quad; unmapped: lo = hi = 0
-                    key[4 * i + 0] = (lo[i] <= 0 && hi[i] > 0) ? (uint32_t)val[i].x : OV_NONE;
-                    key[4 * i + 1] = (lo[i] <= 1 && hi[i] > 1) ? (uint32_t)val[i].y : OV_NONE;
-                    key[4 * i + 2] = (lo[i] <= 2 && hi[i] > 2) ? (uint32_t)val[i].z : OV_NONE;
-                    key[4 * i + 3] = (lo[i] <= 3 && hi[i] > 3) ? (uint32_t)val[i].w : OV_NONE;
+                    if (PAD) {
+                        uint4 q = make_uint4(OV_NONE, OV_NONE, OV_NONE, OV_NONE);
+                        if (qd[i] >= 0) q = __ldg(reinterpret_cast<const uint4*>(H.pcol) + qd[i]);
+                        key[4 * i + 0] = q.x;
+                        key[4 * i + 1] = q.y;
+                        key[4 * i + 2] = q.z;
+                        key[4 * i + 3] = q.w;
+                    } else {
+                        int4 val = make_int4(-1, -1, -1, -1);
+                        if (qd[i] >= 0) {
+                            const int64_t base = (int64_t)qd[i] * 4;
+                            if (base + 3 < H.nnz) {
+                                val = __ldg(reinterpret_cast<const int4*>(col) + qd[i]);
+                            } else {
+                                val.x = base + 0 < H.nnz ? __ldg(col + base + 0) : -1;
+                                val.y = base + 1 < H.nnz ? __ldg(col + base + 1) : -1;
+                                val.z = base + 2 < H.nnz ? __ldg(col + base + 2) : -1;
+                                val.w = base + 3 < H.nnz ? __ldg(col + base + 3) : -1;
+                            }
+                        }
+                        // lo <= 3 and hi >= 1 for every mapped quad; unmapped: lo = hi = 0
+                        key[4 * i + 0] = (lo[i] <= 0 && hi[i] > 0) ? (uint32_t)val.x : OV_NONE;
+                        key[4 * i + 1] = (lo[i] <= 1 && hi[i] > 1) ? (uint32_t)val.y : OV_NONE;
+                        key[4 * i + 2] = (lo[i] <= 2 && hi[i] > 2) ? (uint32_t)val.z : OV_NONE;
+                        key[4 * i + 3] = (lo[i] <= 3 && hi[i] > 3) ? (uint32_t)val.w : OV_NONE;
+                    }
                 }
-                uint32_t c = 0, pend = 0;
+                // home slots first (independent loads), then the rare walks
+                // of flagged homes
+                uint32_t c = 0, pend = 0, pk = 0;
 #pragma unroll
                 for (int t = 0; t < 4 * UNR; ++t) {
                     const uint32_t d = tbl[ov_h1((int32_t)key[t], sh)] ^ key[t];
                     c += (d << 1) == 0u;                       // key bits equal
-                    pend |= (d > OV_FLAG ? 1u : 0u) << t;      // flagged home, other key
+                    const bool f = d > OV_FLAG;                // flagged home, other key
+                    pend |= (f ? 1u : 0u) << t;
+                    pk = f ? key[t] : pk;                      // the last such key
                 }
-                // each lane walks its own flagged homes (usually none or one)
-                while (pend) {
-                    const int t = __ffs(pend) - 1;
-                    pend &= pend - 1u;
-                    uint32_t k = key[0];
+                // each lane walks its own flagged homes: usually none, else
+                // one (pk); several take the general loop
+                if (pend) {
+                    if ((pend & (pend - 1u)) == 0u) {
+                        c += ov_walk(tbl, (int32_t)pk, sh, mask);
+                    } else {
+                        while (pend) {
+                            const int t = __ffs(pend) - 1;
+                            pend &= pend - 1u;
+                            uint32_t k = key[0];
 #pragma unroll
-                    for (int j = 1; j < 4 * UNR; ++j) k = (t == j) ? key[j] : k;
-                    c += ov_walk(tbl, (int32_t)k, sh, mask);
+                            for (int j = 1; j < 4 * UNR; ++j) k = (t == j) ? key[j] : k;
+                            c += ov_walk(tbl, (int32_t)k, sh, mask);
+                        }
+                    }
                 }
                 acc += c;
             }
@@ -1193,11 +1242,18 @@ struct CountWs {
     int32_t* py;              // n_edges (small pairs, then the hub list)
     HubSeg* segs;             // max_segs
     int64_t max_segs;
+    int32_t* pcol;            // padded lists for the hub kernel, pcap entries (null: not carved)
+    int64_t pcap;
     void* tmp;
     size_t tmp_bytes;
 };
 
-static bool carve_count(void* ws, size_t bytes, int64_t n_nodes, int64_t n_edges, CountWs& W, size_t* need) {
+// Padded lists need nnz + 8 (n_nodes + 1) entries; the workspace holds them
+// for nnz <= n_edges (every oriented edge listed once).
+static int64_t pad_capacity(int64_t n_nodes, int64_t nnz) { return nnz + 8 * (n_nodes + 1) + 8; }
+
+static bool carve_count(void* ws, size_t bytes, int64_t n_nodes, int64_t n_edges, CountWs& W, size_t* need,
+                        bool pad = true) {
     const size_t N = (size_t)(n_nodes > 0 ? n_nodes : 0) + 1;
     const size_t E = (size_t)(n_edges > 0 ? n_edges : 1);
     size_t tb = 0;
@@ -1213,6 +1269,8 @@ static bool carve_count(void* ws, size_t bytes, int64_t n_nodes, int64_t n_edges
     // every hub x with pairs opens one segment, every HUB_SEG_MIN pairs at most one more
     W.max_segs = (int64_t)(N < E ? N : E) + (int64_t)(E / HUB_SEG_MIN) + 1;
     W.segs = cv.take<HubSeg>((size_t)W.max_segs);
+    W.pcap = pad ? pad_capacity(n_nodes, (int64_t)E) : 0;
+    W.pcol = pad ? cv.take<int32_t>((size_t)W.pcap) : nullptr;
     W.tmp_bytes = tb;
     W.tmp = cv.take<char>(tb);
     if (need) *need = cv.off;
@@ -1236,9 +1294,9 @@ static int zmask_words(int p) {
 }
 
 static bool carve_count_hybrid(void* ws, size_t bytes, int64_t n_nodes, int64_t n_edges, int64_t zm_rows, int p,
-                               CountWs& W, HybridWs& H, size_t* need) {
+                               CountWs& W, HybridWs& H, size_t* need, bool pad = true) {
     size_t base = 0;
-    carve_count(nullptr, 0, n_nodes, n_edges, W, &base);
+    carve_count(nullptr, 0, n_nodes, n_edges, W, &base, pad);
     const size_t E = (size_t)(n_edges > 0 ? n_edges : 1);
     Carve cv(ws, bytes);
     char* b = cv.take<char>(base);
@@ -1253,7 +1311,7 @@ static bool carve_count_hybrid(void* ws, size_t bytes, int64_t n_nodes, int64_t 
     }
     if (need) *need = cv.off;
     if (!cv.ok()) return false;
-    if (!cv.dry) carve_count(b, base, n_nodes, n_edges, W, nullptr);
+    if (!cv.dry) carve_count(b, base, n_nodes, n_edges, W, nullptr, pad);
     return true;
 }
 
@@ -1383,10 +1441,23 @@ static int launch_hub(const CountParams& P, const CountWs& W, cudaStream_t st, b
     H.seg_ctr = W.ctr + 3;
     H.hub_lg = g_tuning.hub_lg;
     H.result = P.result;
-    auto kern = g_tuning.hub_unroll == 4 ? hub_count_kernel<4> : hub_count_kernel<2>;
+    // padded probe lists when the workspace holds them and quad indices fit int
+    const int64_t need_pad = pad_capacity(P.n_nodes, P.nnz);
+    const bool pad = W.pcol != nullptr && need_pad <= W.pcap && need_pad <= (int64_t)INT32_MAX;
+    H.pcol = pad ? W.pcol : nullptr;
+    if (pad) {
+        int64_t g = (P.n_nodes + 31) / 32;
+        const int64_t cap = (int64_t)sm_count() * 16;
+        g = g < 1 ? 1 : (g > cap ? cap : g);
+        pad_rows_kernel<<<(int)g, 256, 0, st>>>(P.row_ptr, P.n_nodes, P.col_idx, W.pcol);
+        TCHLL_CHECK_LAUNCH("pad_rows_kernel");
+    }
+    const int vi = (g_tuning.hub_unroll == 4 ? 2 : 0) + (pad ? 1 : 0);
+    auto kern = vi == 3 ? hub_count_kernel<4, true>
+                        : vi == 2 ? hub_count_kernel<4, false> : vi == 1 ? hub_count_kernel<2, true> : hub_count_kernel<2, false>;
     const size_t smem = sizeof(int32_t) << g_tuning.hub_lg;
-    static size_t smem_set[2] = {0, 0};
-    size_t& done = smem_set[g_tuning.hub_unroll == 4 ? 1 : 0];
+    static size_t smem_set[4] = {0, 0, 0, 0};
+    size_t& done = smem_set[vi];
     cudaError_t e;
     if (smem > done) {
         e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1427,14 +1498,17 @@ static int run_count(CountParams P, int mode, bool details, void* ws, size_t ws_
     HybridWs HW{};
     size_t need = 0;
     bool ok;
+    // Optional parts, used when the workspace has room (same results): the
+    // padded probe lists of the hub kernel and, for hybrid calls, the zero
+    // masks that let the HLL pass test linear counting without the registers.
     if (mode == MODE_EXACT) {
-        ok = carve_count(ws, ws_bytes, P.n_nodes, P.n_edges, W, &need);
+        ok = carve_count(ws, ws_bytes, P.n_nodes, P.n_edges, W, &need, true);
+        if (!ok) ok = carve_count(ws, ws_bytes, P.n_nodes, P.n_edges, W, &need, false);
     } else {
-        // With room for the zero masks the HLL pass reads them instead of
-        // the registers for the linear-counting test (same results).
         const int64_t zm_rows = P.slot ? P.n_rows : P.n_nodes;
         ok = zm_rows > 0 && carve_count_hybrid(ws, ws_bytes, P.n_nodes, P.n_edges, zm_rows, P.p, W, HW, &need);
-        if (!ok) ok = carve_count_hybrid(ws, ws_bytes, P.n_nodes, P.n_edges, 0, P.p, W, HW, &need);
+        if (!ok) ok = carve_count_hybrid(ws, ws_bytes, P.n_nodes, P.n_edges, 0, P.p, W, HW, &need, true);
+        if (!ok) ok = carve_count_hybrid(ws, ws_bytes, P.n_nodes, P.n_edges, 0, P.p, W, HW, &need, false);
     }
     if (!ok || ws == nullptr) {
         set_error("workspace too small: need %zu bytes, have %zu", need, ws_bytes);
@@ -1781,7 +1855,7 @@ TCHLL_EXPORT int tchll_exact_count_noalloc(const int32_t* row_ptr, int64_t n_nod
     if (rc) return rc;
     CountWs W;
     size_t need = 0;
-    carve_count(nullptr, 0, n_nodes, n_edges, W, &need);
+    carve_count(nullptr, 0, n_nodes, n_edges, W, &need, false);  // padded lists only when they fit too
     if (need > (size_t)TCHLL_NOALLOC_SCRATCH_BYTES) {
         set_error("graph too large for tchll_exact_count_noalloc: needs %zu bytes of scratch (about 8 per edge + "
                   "32 per vertex), the fixed limit is %u bytes; use tchll_exact_count with a workspace",
