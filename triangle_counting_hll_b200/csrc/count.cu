@@ -747,12 +747,16 @@ __global__ void __launch_bounds__(256, 5) hub_count_kernel(const HubParams H) {
             __syncthreads();
         }
         const bool table = fits && !s_fail;  // CTA-uniform
+        // pairs per round: up to 32, fewer for short segments so that every
+        // warp of the CTA gets about two rounds
+        int rsz = (sg.len + 15) >> 4;
+        rsz = rsz < 4 ? 4 : (rsz > 32 ? 32 : rsz);
         while (true) {
             int r = 0;
-            if (lane == 0) r = atomicAdd(&s_round, 32);
+            if (lane == 0) r = atomicAdd(&s_round, rsz);
             r = __shfl_sync(FULL, r, 0);
             if (r >= sg.len) break;
-            const int np = min(32, sg.len - r);
+            const int np = min(rsz, sg.len - r);
             int32_t rs = 0, re = 0, vs = 0, ve = 0;
             if (lane < np) {
                 const int32_t y = __ldg(H.hy + sg.start + r + lane);
@@ -1172,7 +1176,7 @@ struct Tuning {
     int warps = 8;          // warps per CTA
     int pairs = 1;          // table-side / probe-side reorientation
     int sparse = 0;         // table load <= 1/4 where it fits
-    int hub = 256;          // pairs with d+(x) > hub go to the CTA-table kernel (0: off)
+    int hub = 128;          // pairs with d+(x) > hub go to the CTA-table kernel (0: off)
     int hub_seg = 2048;     // hub pairs per CTA work unit
     int hub_lg = 13;        // largest CTA table: 2^13 slots = 32 KB
     int hub_unroll = 2;     // quads per lane in flight (2 or 4)
