@@ -92,6 +92,7 @@ struct CountParams {
     const int32_t* chunk_graph;
     const int64_t* n_chunks_dev;
     const int32_t* graph_vbase;  // vertex range of graph g: [vbase[g], vbase[g+1])
+    int64_t n_graphs;            // batched calls: graphs in graph_vbase (else 0)
     // Hybrid with pairs: the routing pass appends HLL edges here
     int32_t* hll_u;
     int32_t* hll_v;
@@ -219,6 +220,16 @@ __device__ __forceinline__ bool pair_of(const CountParams& P, int64_t e, int32_t
     return true;
 }
 
+// Batched calls: the graph of vertex v, the last g with vbase[g] <= v.
+__device__ __forceinline__ int64_t graph_of(const int32_t* vbase, int64_t n_graphs, int32_t v) {
+    int64_t lo = 0, hi = n_graphs - 1;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi + 1) >> 1;
+        if (__ldg(vbase + mid) <= v) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
 template <bool HYB>
 __global__ void pair_hist_kernel(const CountParams P, int32_t* cnt) {
     uint32_t status = 0;
@@ -235,7 +246,12 @@ __global__ void pair_hist_kernel(const CountParams P, int32_t* cnt) {
             bool wants, both;
             ok = route(P, u, v, du, dv, su, sv, wants, both, status);
             hll = ok && wants && both;
-            fallback += (ok && wants && !both);
+            if (ok && wants && !both) {
+                if (P.graph_vbase && P.hll_u)  // batched: this edge's graph
+                    atomicAdd((unsigned long long*)&P.result[graph_of(P.graph_vbase, P.n_graphs, u)].n_fallback, 1ull);
+                else
+                    ++fallback;
+            }
         }
         if (ok && !hll) atomicAdd(cnt + (((ue - us) >= (ve - vs)) ? u : v), 1);
         if (HYB && P.hll_u) {
@@ -974,6 +990,8 @@ struct HllParams {
     const int64_t* slot;  // null: dense rows (row v at v * 2^p)
     const uint32_t* zm;   // zero masks, zst words per row (null: count zeros from the registers)
     int zst;
+    const int32_t* vbase;  // batched: per-edge results go to result[graph of u]
+    int64_t n_graphs;
     int p;
     int variant;
     uint32_t lc_min;
@@ -1159,9 +1177,20 @@ __global__ void __launch_bounds__(256) hll_edges_kernel(const HllParams H) {
             // max(0.0, min(s_hat, upper)) with Python's min/max argument order
             double s_cl = (upper < s_hat) ? upper : s_hat;
             s_cl = (s_cl > 0.0) ? s_cl : 0.0;
-            if (s_hat < 0.0 || s_hat > upper) ++n_clamped;
-            ++n_approx;
-            hacc.add((uint64_t)__double2ull_rn(s_cl * 4294967296.0));
+            const bool clamped = s_hat < 0.0 || s_hat > upper;
+            const uint64_t fx = (uint64_t)__double2ull_rn(s_cl * 4294967296.0);
+            if (H.vbase) {  // batched: straight into this edge's graph
+                tchll_count_result* R = H.result + graph_of(H.vbase, H.n_graphs, u);
+                U128 one;
+                one.lo = fx;
+                atomic_add_u128((unsigned long long*)&R->hll_fx_lo, one);
+                atomicAdd((unsigned long long*)&R->n_approx, 1ull);
+                if (clamped) atomicAdd((unsigned long long*)&R->n_clamped, 1ull);
+            } else {
+                n_clamped += clamped;
+                ++n_approx;
+                hacc.add(fx);
+            }
         }
     }
     publish(H.result, 0, hacc, n_approx, 0, 0, n_clamped, 0u, lane);
@@ -1341,6 +1370,8 @@ static int launch_hll_edges_L(const HllParams& H, cudaStream_t st) {
 
 static int launch_hll_edges(const CountParams& P, const HybridWs& HW, cudaStream_t st) {
     HllParams H;
+    H.vbase = P.graph_vbase;
+    H.n_graphs = P.n_graphs;
     H.hu = HW.hll_u;
     H.hv = HW.hll_v;
     H.n_dev = HW.hll_n;
@@ -1947,6 +1978,7 @@ __global__ void check_vbase_kernel(const int32_t* __restrict__ vbase, int64_t n_
 
 struct BatchWs {
     CountWs cw;
+    HybridWs hw;      // HLL edge list (no zero masks)
     int64_t* cnt;     // n_graphs + 1
     int64_t* coff;    // n_graphs + 1 (last entry: number of chunks)
     int64_t* cstart;  // max chunks
@@ -1977,6 +2009,12 @@ static bool carve_batch(void* ws, size_t bytes, int64_t n_nodes, int64_t n_edges
     B.cgraph = cv.take<int32_t>(MC);
     B.tmp_bytes = tb;
     B.tmp = cv.take<char>(tb);
+    const size_t E = (size_t)(n_edges > 0 ? n_edges : 1);
+    B.hw.hll_u = cv.take<int32_t>(E);
+    B.hw.hll_v = cv.take<int32_t>(E);
+    B.hw.hll_n = cv.take<unsigned long long>(1);
+    B.hw.zm = nullptr;
+    B.hw.zst = 0;
     if (need) *need = cv.off;
     if (!cv.ok() || cv.dry) return cv.ok();
     carve_count(cbase, cneed, n_nodes, n_edges, B.cw, nullptr);
@@ -2026,6 +2064,7 @@ static int run_batch(CountParams P, bool hybrid, const int32_t* vbase, int64_t n
     P.sparse = g_tuning.sparse;
     P.n_edges_dev = nullptr;
     P.graph_vbase = vbase;
+    P.n_graphs = n_graphs;
     P.n_chunks_dev = B.coff + n_graphs;
     P.chunk_start = B.cstart;
     P.chunk_len = B.clen;
@@ -2035,6 +2074,14 @@ static int run_batch(CountParams P, bool hybrid, const int32_t* vbase, int64_t n
     CountParams Q;
     phase_reset();
     P.work = B.cw.ctr;
+    // Hybrid: the routing pass also appends the HLL-routed edges to a list
+    // (16-byte aligned register rows; else the HLL edges take a second pass
+    // over each graph's edges below).
+    const bool hll_list = hybrid && ((uintptr_t)P.regs % 16 == 0);
+    P.hll_u = hll_list ? B.hw.hll_u : nullptr;
+    P.hll_v = hll_list ? B.hw.hll_v : nullptr;
+    P.hll_n = hll_list ? B.hw.hll_n : nullptr;
+    if (hll_list) TCHLL_CUDA(cudaMemsetAsync(B.hw.hll_n, 0, sizeof(unsigned long long), st));
     phase_mark(0, st);
     // pairs with a long table side go to the hub kernel, which publishes
     // per segment into the graph of x
@@ -2049,6 +2096,7 @@ static int run_batch(CountParams P, bool hybrid, const int32_t* vbase, int64_t n
     if (rc) return rc;
     phase_mark(1, st);
     Q.n_edges_dev = nullptr;
+    Q.hll_u = nullptr;
     rc = launch_count<MODE_EXACT>(Q, false, st);
     if (rc) return rc;
     if (hub > 0) {
@@ -2058,6 +2106,12 @@ static int run_batch(CountParams P, bool hybrid, const int32_t* vbase, int64_t n
     phase_mark(2, st);
     g_phase.used[0] = g_phase.used[1] = true;
     if (!hybrid) return TCHLL_OK;
+    if (hll_list) {  // per-edge estimates into each edge's graph
+        rc = launch_hll_edges(P, B.hw, st);
+        phase_mark(3, st);
+        g_phase.used[2] = true;
+        return rc;
+    }
     // HLL-routed edges: chunks over each graph's CSR edge range
     TCHLL_CUDA(cudaMemsetAsync(B.cw.ctr + 1, 0, sizeof(unsigned long long), st));
     rc = build_chunks(P.row_ptr, vbase, n_graphs, P.n_nodes, B, st);
