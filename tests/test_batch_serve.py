@@ -147,8 +147,7 @@ def test_captured_batch_replays_and_tuning(tchll):
         t3, s3 = bt.hybrid_counts(8, 8, 10)
         assert np.array_equal(t1, t2) and np.array_equal(t1, t3)
     finally:
-        core.set_count_tuning(**{k: base[k] for k in ("chunk", "slots_log2", "tiny", "blocks_per_sm", "warps",
-                                                       "pairs", "sparse")})
+        core.set_count_tuning(**base)
 
 
 @pytest.mark.gpu

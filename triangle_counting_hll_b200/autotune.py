@@ -25,12 +25,16 @@ from . import _lib, core
 from ._lib import check, load, ptr, stream_handle
 
 CANDIDATES: List[Dict] = [
-    {"chunk": 256, "slots_log2": 11, "tiny": 16, "sparse": 0},
-    {"chunk": 128, "slots_log2": 11, "tiny": 16, "sparse": 0},
-    {"chunk": 512, "slots_log2": 11, "tiny": 16, "sparse": 0},
-    {"chunk": 256, "slots_log2": 11, "tiny": 48, "sparse": 1},
-    {"chunk": 256, "slots_log2": 10, "tiny": 24, "sparse": 0},
-    {"chunk": 64, "slots_log2": 9, "tiny": 32, "sparse": 0},
+    {"chunk": 256, "slots_log2": 11, "tiny": 16, "sparse": 0, "hub": 128},
+    {"chunk": 128, "slots_log2": 11, "tiny": 16, "sparse": 0, "hub": 128},
+    {"chunk": 512, "slots_log2": 11, "tiny": 16, "sparse": 0, "hub": 128},
+    {"chunk": 256, "slots_log2": 11, "tiny": 48, "sparse": 1, "hub": 128},
+    {"chunk": 256, "slots_log2": 10, "tiny": 24, "sparse": 0, "hub": 128},
+    {"chunk": 64, "slots_log2": 9, "tiny": 32, "sparse": 0, "hub": 128},
+    {"chunk": 256, "slots_log2": 11, "tiny": 16, "sparse": 0, "hub": 256},
+    {"chunk": 256, "slots_log2": 10, "tiny": 24, "sparse": 0, "hub": 256},
+    {"chunk": 256, "slots_log2": 11, "tiny": 16, "sparse": 0, "hub": 0},
+    {"chunk": 256, "slots_log2": 10, "tiny": 24, "sparse": 0, "hub": 0},
 ]
 
 
@@ -84,7 +88,7 @@ class Autotuner:
     @staticmethod
     def apply(cfg: Dict) -> None:
         core.set_count_tuning(chunk=cfg["chunk"], slots_log2=cfg["slots_log2"], tiny=cfg["tiny"],
-                              sparse=bool(cfg.get("sparse", 0)))
+                              sparse=bool(cfg.get("sparse", 0)), hub=int(cfg.get("hub", 128)))
 
     def tune(self, key_row_ptr: torch.Tensor, run: Callable[[], None], reps: int = 2) -> Dict:
         """Pick (or recall) the fastest candidate for graphs shaped like the one

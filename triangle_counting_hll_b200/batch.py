@@ -276,6 +276,15 @@ def bench_entry(dev, quick: bool = True, n_graphs: int = 2048, theta: int = 64, 
     out: Dict = {"n_graphs": n_graphs, "n_edges": batch.csr.n_edges, "theta": theta, "gamma": theta, "p": p,
                  "sizes": "lognormal median 5000 sigma 1.0 clipped [500, 500000]; even ER, odd Chung-Lu 2.1; deg 12"}
     reps = 3 if quick else 10
+    base = core.get_count_tuning()
+    try:
+        return _bench_modes(dev, batch, csrs, out, reps, theta, p)
+    finally:  # the tuning is process-wide: leave it as it was
+        core.set_count_tuning(**base)
+
+
+def _bench_modes(dev, batch, csrs, out: Dict, reps: int, theta: int, p: int) -> Dict:
+    n_graphs = batch.n_graphs
     tuned = autotune.tune_batch(batch)
     out["tuning"] = tuned
     plain_sk = plain_sketches(csrs, theta, p)
