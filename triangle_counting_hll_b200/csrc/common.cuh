@@ -44,6 +44,15 @@ void count_launch(int n = 1);
 
 int sm_count();
 
+// Current device ordinal, or -1 if it cannot be read or is >= kMaxDevices
+// (per-device host caches are indexed by it).
+constexpr int kMaxDevices = 64;
+inline int current_device() {
+    int d = -1;
+    if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= kMaxDevices) return -1;
+    return d;
+}
+
 // Workspace carving: bump allocator over a caller-provided buffer.
 struct Carve {
     char* base;

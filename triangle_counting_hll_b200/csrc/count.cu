@@ -253,7 +253,13 @@ __global__ void pair_hist_kernel(const CountParams P, int32_t* cnt) {
                     ++fallback;
             }
         }
-        if (ok && !hll) atomicAdd(cnt + (((ue - us) >= (ve - vs)) ? u : v), 1);
+        {
+            // lanes with the same table side (consecutive CSR edges share u)
+            // add with one atomic
+            const int32_t x = (ok && !hll) ? (((ue - us) >= (ve - vs)) ? u : v) : -1;
+            const unsigned peers = __match_any_sync(__activemask(), x);
+            if (x >= 0 && lane == __ffs(peers) - 1) atomicAdd(cnt + x, __popc(peers));
+        }
         if (HYB && P.hll_u) {
             // warp-aggregated append of the HLL-routed edges
             const unsigned act = __activemask();
@@ -281,15 +287,25 @@ template <bool HYB>
 __global__ void pair_scatter_kernel(const CountParams P, int32_t* cursor, int32_t* cursorh, int hub,
                                     const int32_t* n_small, int32_t* px, int32_t* py) {
     uint32_t status = 0;
+    const int lane = threadIdx.x & 31;
     const int64_t hbase = hub > 0 ? (int64_t)*n_small : 0;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < P.n_edges;
          e += (int64_t)gridDim.x * blockDim.x) {
-        int32_t x, y, xl;
-        if (pair_of<HYB>(P, e, x, y, xl, status)) {
-            if (hub > 0 && xl > hub) {
-                py[hbase + atomicAdd(cursorh + x, 1)] = y;
+        int32_t x = 0, y = 0, xl = 0;
+        const bool ok = pair_of<HYB>(P, e, x, y, xl, status);
+        // lanes with the same x claim their positions with one atomic (x's
+        // list length, hence its list, is the same for all of them)
+        const unsigned peers = __match_any_sync(__activemask(), ok ? x : -1);
+        if (ok) {
+            const int leader = __ffs(peers) - 1;
+            const bool to_hub = hub > 0 && xl > hub;
+            int32_t base = 0;
+            if (lane == leader) base = atomicAdd((to_hub ? cursorh : cursor) + x, __popc(peers));
+            base = __shfl_sync(peers, base, leader);
+            const int32_t pos = base + __popc(peers & ((1u << lane) - 1u));
+            if (to_hub) {
+                py[hbase + pos] = y;
             } else {
-                const int32_t pos = atomicAdd(cursor + x, 1);
                 px[pos] = x;
                 py[pos] = y;
             }
@@ -1239,12 +1255,16 @@ static int launch_mode(const CountParams& P, cudaStream_t st) {
     auto kern = count_kernel<MODE, VEC, DETAILS>;
     const int threads = g_tuning.warps * 32;
     const size_t smem = (size_t)g_tuning.warps * ((size_t)1 << P.slots_log2) * sizeof(int32_t);
-    static size_t smem_set = 0;  // largest dynamic smem opted into so far
+    // largest dynamic smem opted into so far, per device (the attribute is
+    // per device; a process may drive several)
+    static size_t smem_set[kMaxDevices] = {};
+    const int dev = current_device();
     cudaError_t e;
-    if (smem > smem_set) {
+    if (dev < 0) return cuda_status(cudaErrorInvalidDevice, "cudaGetDevice");
+    if (smem > smem_set[dev]) {
         e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(count_kernel)");
-        smem_set = smem;
+        smem_set[dev] = smem;
     }
     int bps = g_tuning.blocks_per_sm;
     if (bps <= 0) {
@@ -1491,8 +1511,10 @@ static int launch_hub(const CountParams& P, const CountWs& W, cudaStream_t st, b
     auto kern = vi == 3 ? hub_count_kernel<4, true>
                         : vi == 2 ? hub_count_kernel<4, false> : vi == 1 ? hub_count_kernel<2, true> : hub_count_kernel<2, false>;
     const size_t smem = sizeof(int32_t) << g_tuning.hub_lg;
-    static size_t smem_set[4] = {0, 0, 0, 0};
-    size_t& done = smem_set[vi];
+    static size_t smem_set[kMaxDevices][4] = {};  // per device and kernel variant
+    const int dev = current_device();
+    if (dev < 0) return cuda_status(cudaErrorInvalidDevice, "cudaGetDevice");
+    size_t& done = smem_set[dev][vi];
     cudaError_t e;
     if (smem > done) {
         e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -169,10 +169,12 @@ static int launch_sketch(const int32_t* row_ptr, int64_t n, const int32_t* col_i
     if (n == 0) return TCHLL_OK;
     auto kern = sketch_kernel<DENSE>;
     const size_t smem = (size_t)1 << p;
-    static size_t smem_set = 0;
-    if (smem > smem_set) {
+    static size_t smem_set[kMaxDevices] = {};  // per device: the attribute is per device
+    const int dev = current_device();
+    if (dev < 0) return cuda_status(cudaErrorInvalidDevice, "cudaGetDevice");
+    if (smem > smem_set[dev]) {
         TCHLL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        smem_set = smem;
+        smem_set[dev] = smem;
     }
     int bps = 1;
     TCHLL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, kSketchThreads, smem));
