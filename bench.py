@@ -303,7 +303,9 @@ def run_ours(args):
         "clocks": clk,
     }
 
-    if not args.no_extras:
+    # the extras (hybrid sweep, batched and serving workloads) are one-GPU
+    # measurements: a multi-GPU run reports the headline line only
+    if not args.no_extras and world == 1:
         line["hybrid"] = hybrid_sweep(g, count, dev)
         for name, mod in (("batched", "triangle_counting_hll_b200.batch"),
                           ("serving", "triangle_counting_hll_b200.serve")):
