@@ -45,7 +45,7 @@ WORKLOAD = "rmat22_ef16_exact_count"
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--scale", type=int, default=SCALE)
@@ -94,7 +94,7 @@ def load_traffic(workload: str):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms while active."""
+    """nvidia-smi clocks / throttle reasons sampled every 100 ms while active."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -111,7 +111,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
 
@@ -536,7 +536,10 @@ def run_reference(args):
     rp, ci, eu, ev = g["row_ptr"], g["col_idx"], g["edge_u"], g["edge_v"]
     E = len(eu)
     rate = calibrate_rate(O, rp, ci, eu, ev, cores)
-    stride = max(int(E // max(rate * 3.0, 1.0)), 1)  # about 3 s of CPU work per step
+    # about 3 s of CPU work per step, less when many steps are asked for, so
+    # the whole run stays near a minute of CPU time
+    per_step = min(3.0, max(0.5, 60.0 / max(args.steps + args.warmup, 1)))
+    stride = max(int(E // max(rate * per_step, 1.0)), 1)
     sel = np.arange(0, E, stride)
     su, sv = eu[sel], ev[sel]
     for _ in range(max(args.warmup, 0)):
