@@ -722,16 +722,24 @@ __device__ __forceinline__ int64_t pad_start(int32_t rs, int32_t y) {
 
 __global__ void pad_rows_kernel(const int32_t* __restrict__ row_ptr, int64_t n_nodes,
                                 const int32_t* __restrict__ col, int32_t* __restrict__ pcol) {
-    const int sub = threadIdx.x & 7;  // 8 lanes per row
+    const int sub = threadIdx.x & 7;  // 8 lanes per row, one 16-byte quad each
     const int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 3;
     const int64_t ng = ((int64_t)gridDim.x * blockDim.x) >> 3;
     for (int64_t y = g; y < n_nodes; y += ng) {
         const int32_t rs = __ldg(row_ptr + y);
         const int32_t d = __ldg(row_ptr + y + 1) - rs;
         if (d <= 0) continue;
-        const int64_t ps = pad_start(rs, (int32_t)y);
-        const int32_t len = (d + 3) & ~3;
-        for (int32_t i = sub; i < len; i += 8) pcol[ps + i] = i < d ? __ldg(col + rs + i) : (int32_t)OV_NONE;
+        const int64_t ps = pad_start(rs, (int32_t)y);  // a multiple of 4: 16-byte aligned stores
+        const int32_t nq = (d + 3) >> 2;
+        for (int32_t q = sub; q < nq; q += 8) {
+            const int32_t i = 4 * q;
+            int4 w;
+            w.x = __ldg(col + rs + i);  // i < d
+            w.y = i + 1 < d ? __ldg(col + rs + i + 1) : (int32_t)OV_NONE;
+            w.z = i + 2 < d ? __ldg(col + rs + i + 2) : (int32_t)OV_NONE;
+            w.w = i + 3 < d ? __ldg(col + rs + i + 3) : (int32_t)OV_NONE;
+            *reinterpret_cast<int4*>(pcol + ps + i) = w;
+        }
     }
 }
 
