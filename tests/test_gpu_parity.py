@@ -3,7 +3,7 @@ CPU oracle and the golden fixtures recorded from the reference.
 
 Bit-exact: CSR arrays, exact counts, HLL registers, routing stats.
 Tolerance: hybrid totals within 1e-9 relative of the FP64 oracle (the
-north-star bar is 1e-6), single estimates within 1e-12 relative.
+required bar is 1e-6), single estimates within 1e-12 relative.
 """
 from __future__ import annotations
 

@@ -1,6 +1,6 @@
 """The reference's other estimators, on the GPU, for comparison runs.
 
-The north-star estimator is src/hll.py + src/hybrid.py (modules ``hll`` and
+The main estimator is src/hll.py + src/hybrid.py (modules ``hll`` and
 ``hybrid``).  The reference's CPU experiment (cpu_exp/triangle_hll_
 experiment.py) uses a different HLL variant, and its published CPU numbers
 are quoted with it: splitmix64 with the +0x9E3779B97F4A7C15 increment and a
