@@ -1087,7 +1087,7 @@ __device__ __forceinline__ void hll_word128(uint32_t w, int S, U128& sum, double
 }
 
 template <int L, bool ZM, bool CACHE>
-__global__ void __launch_bounds__(256) hll_edges_kernel(const HllParams H) {
+__global__ void __launch_bounds__(256, CACHE ? 3 : 4) hll_edges_kernel(const HllParams H) {
     const int lane = threadIdx.x & 31;
     const int sub = lane & (L - 1);
     const unsigned gmask = (L == 32) ? FULL : (((1u << L) - 1u) << (lane & ~(L - 1)));
