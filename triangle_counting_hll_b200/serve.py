@@ -445,6 +445,9 @@ def bench_entry(dev, quick: bool = True) -> Dict:
     for _ in range(2):
         Server(dev, budget_bytes=120e9).serve(warm)
         serve_sequential(warm, dev)
+    # and one paced run like the timed ones (other graphs), so the server's
+    # streams have served requests arriving one at a time too
+    Server(dev, budget_bytes=120e9).serve(c5_requests(60, 50.0, seed=4242))
     torch.cuda.synchronize(dev)
     for rate in (50.0, 200.0, 1000.0):
         reqs = c5_requests(n, rate, seed=int(rate))
