@@ -37,6 +37,7 @@ extern "C" {
 #define TCHLL_STATUS_BAD_EDGE 1u /* edge endpoint outside [0, n_nodes) */
 #define TCHLL_STATUS_BAD_ROW 2u  /* row_ptr extent outside [0, nnz] or decreasing */
 #define TCHLL_STATUS_BAD_SLOT 4u /* sketch slot outside [0, n_rows) */
+#define TCHLL_STATUS_BAD_KEY 8u  /* neighbour id (col_idx value) outside [0, n_nodes) */
 
 /*
  * Totals written by the counting entry points (64 bytes, device memory).
@@ -156,6 +157,29 @@ int tchll_get_count_tuning(int32_t* out8 /* host */);
 int tchll_set_count_hub(int32_t threshold, int32_t seg_pairs, int32_t table_log2, int32_t unroll);
 int tchll_get_count_hub(int32_t* out4 /* host */);
 
+/* Hub core (pairs layout, with the padded lists in the workspace): the hub
+ * kernels work in the coordinates of the core, the vertices that appear in
+ * some hub table side's forward list, and probe only the core members of
+ * each probe list; when the core fits 8 * 2^bitmap_log2 bits of shared
+ * memory (minus 32), a table side's list is a bitmap there, else a hash
+ * table.  bitmap_log2 0 always uses hash tables; otherwise in [10, 17].
+ * overlap != 0 runs a hybrid count's HLL pass on a second stream beside the
+ * exact pairs (joined before the call returns).  out2 receives the two
+ * values.  Results are identical for every setting.  These kernels read
+ * col_idx values as vertex indices: a value outside [0, n_nodes) is
+ * reported as TCHLL_STATUS_BAD_KEY. */
+int tchll_set_count_core(int32_t bitmap_log2, int32_t overlap);
+int tchll_get_count_core(int32_t* out2 /* host */);
+
+/* HLL pass of the hybrid counts: for p <= onepass_max_p one pass over both
+ * register rows of an edge forms the zero count and the exact sum of 2^-r
+ * together; above it the rows' zero masks are read first and the registers
+ * only when linear counting cannot apply.  lanes: lanes per HLL edge (0:
+ * chosen by p, else a power of two in [1, 32]).  out2 receives both values.
+ * Results are identical for every setting. */
+int tchll_set_hll_pass(int32_t onepass_max_p, int32_t lanes);
+int tchll_get_hll_pass(int32_t* out2 /* host */);
+
 /*
  * Allocation-free exact count, for callers that cannot allocate device memory
  * (a binding with no CUDA allocator of its own, or a service whose device
@@ -167,8 +191,10 @@ int tchll_get_count_hub(int32_t* out4 /* host */);
  * lists, four per-vertex histograms / offsets and the work-unit list, so for
  * example 3 M edges on 200 K vertices fit) are rejected with TCHLL_EINVAL.
  * The first
- * call on a device looks up the array's device address; make that first call
- * before any stream capture.  All calls share the one array: calls that
+ * call in each CUDA context looks up the array's device address (cached per
+ * context id, so a context made current by the caller, or one re-created
+ * after cudaDeviceReset, gets its own lookup); make that first call before
+ * any stream capture.  All calls share the one array: calls that
  * overlap on the GPU (different streams or devices sharing a context) race;
  * serialize them.  Nothing here calls cudaMalloc or cudaFree.
  */
@@ -181,12 +207,15 @@ int tchll_exact_count_noalloc(const int32_t* row_ptr, int64_t n_nodes, const int
  * When enabled, the counting entry points record CUDA events on the
  * caller's stream around their phases; tchll_phase_times then waits for the
  * last call's events and writes milliseconds: ms3[0] pair regrouping,
- * ms3[1] exact-count kernels (pair kernel and hub kernel), ms3[2] HLL kernel
- * (-1 for a phase the call did not run).  tchll_phase_hub_ms writes the hub
- * kernel's share of ms3[1] (-1 when it did not run). */
+ * ms3[1] exact-count kernels (pair kernel and hub kernels), ms3[2] HLL pass
+ * (-1 for a phase the call did not run; with the overlap on, the HLL pass
+ * runs beside ms3[1] on the second stream).  tchll_phase_hub_ms writes the
+ * hub pairs' share of ms3[1]: ms2[0] the hub kernels, ms2[1] the core pass
+ * before them (-1 when they did not run).  While timing is on, counting
+ * calls serialize their enqueues. */
 int tchll_set_phase_timing(int32_t enable);
 int tchll_phase_times(float* ms3 /* host */);
-int tchll_phase_hub_ms(float* ms /* host */);
+int tchll_phase_hub_ms(float* ms2 /* host */);
 
 /* ------------------------------------------------------------ sketches --- */
 /*
@@ -304,7 +333,10 @@ int tchll_degree_stats(const int32_t* degrees, const int32_t* row_ptr, int64_t n
  *   degrees (forward)[n_nodes], node_ids (original id)[n_nodes] and, when
  *   undirected_degrees is not NULL, the undirected degree[n_nodes]
  *   (orient_graph's degree dict, src/graph.py:41-44).
- * Negative ids are TCHLL_EINVAL via sizes[0] = -1.
+ * Negative ids are TCHLL_EINVAL via sizes[0] = -1.  Phase 1 waits for the
+ * stream once, early, to read the largest id (16 bytes): it sets the width of
+ * the sort keys and, when ids 0 .. max fit twice n_raw entries, lets a direct
+ * rank table replace the sort of all endpoints.
  */
 int tchll_csr_workspace_bytes(int64_t n_raw, size_t* bytes);
 int tchll_csr_build_phase1(const int32_t* raw_u, const int32_t* raw_v, int64_t n_raw, int64_t* sizes,

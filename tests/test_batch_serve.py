@@ -102,11 +102,29 @@ def test_batched_hub_segments_go_to_their_graph(tchll, oracle):
     assert np.array_equal(tot, rtot)
     for k in rst:
         assert np.array_equal(st[k], rst[k]), k
+    for i in (2, 5, 10):  # the 300-clique, the R-MAT graph, the 400-clique
+        a, b, _ = items[i]
+        otot, ost = _oracle_hybrid(oracle, a.cpu().numpy(), b.cpu().numpy(), 64, 64, 10)
+        assert tot[i] == pytest.approx(otot, rel=1e-9) and st["n_approx"][i] == ost["n_approx"], i
+
+
+def _oracle_hybrid(oracle, u, v, theta, gamma, p):
+    """The oracle's hybrid total and stats of one graph given by its raw
+    endpoint arrays (CSR build, compact sketches of rows >= theta, route by
+    gamma)."""
+    og = oracle.csr_build(u, v)
+    if og["n_edges"] == 0:
+        return 0.0, {"n_approx": 0, "n_exact": 0, "n_fallback": 0, "n_clamped": 0}
+    oslot, orows = oracle.build_sketches_compact(og["row_ptr"].astype(np.int64), og["col_idx"].astype(np.int64),
+                                                 theta, p)
+    otot, ost, _ = oracle.hybrid_count(og["row_ptr"], og["col_idx"], og["edge_u"], og["edge_v"], og["degrees"],
+                                       oslot, orows, p, gamma)
+    return otot, ost
 
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("theta,p", [(8, 10), (16, 8), (4, 12)])
-def test_batched_hybrid_bit_exact_vs_one_at_a_time(tchll, theta, p):
+def test_batched_hybrid_bit_exact_vs_one_at_a_time(tchll, oracle, theta, p):
     import torch
     from triangle_counting_hll_b200 import batch as B
     from triangle_counting_hll_b200 import core
@@ -120,6 +138,13 @@ def test_batched_hybrid_bit_exact_vs_one_at_a_time(tchll, theta, p):
     for k in rst:
         assert np.array_equal(st[k], rst[k]), k
     assert st["n_approx"].sum() > 0  # the HLL path ran
+    # and each graph's total and stats against the oracle's FP64 evaluation of
+    # the reference estimator on that graph alone
+    for i, (u, v, _) in enumerate(items):
+        otot, ost = _oracle_hybrid(oracle, u.cpu().numpy(), v.cpu().numpy(), theta, theta, p)
+        assert tot[i] == pytest.approx(otot, rel=1e-9, abs=1e-9), i
+        assert (st["n_approx"][i], st["n_exact"][i], st["n_clamped"][i]) == \
+            (ost["n_approx"], ost["n_exact"], ost["n_clamped"]), i
     ex = bt.exact_counts()
     assert np.array_equal(st["n_approx"] + st["n_exact"], np.array([c.n_edges for c in csrs]))
     assert (tot[st["n_approx"] == 0] == ex[st["n_approx"] == 0]).all()
@@ -191,7 +216,7 @@ def _serve_mix(dev, n=60, rate=400.0, budget=120e9, scale_range=(8, 12), repeat=
 
 
 @pytest.mark.gpu
-def test_server_results_same_alone_and_in_the_mix(tchll):
+def test_server_results_same_alone_and_in_the_mix(tchll, oracle):
     import torch
     from triangle_counting_hll_b200 import serve as S
     dev = torch.device("cuda", 0)
@@ -206,6 +231,16 @@ def test_server_results_same_alone_and_in_the_mix(tchll):
     for r, c in zip(sorted(reqs, key=lambda r: r.rid), got):
         alone = S.answer_alone(r, dev)
         assert c.value == alone.value and c.stats == alone.stats, r  # bit-identical, exact and hybrid
+        # and against the oracle on the same request graph (the oracle's
+        # generator draws the same edges as the device one)
+        ou, ov = oracle.gen_rmat(r.scale, r.edge_factor, *S.RMAT_ABC, r.seed)
+        if r.mode == "exact":
+            og = oracle.csr_build(ou, ov)
+            assert c.value == oracle.exact_count(og["row_ptr"], og["col_idx"], og["edge_u"], og["edge_v"]), r
+        else:
+            otot, ost = _oracle_hybrid(oracle, ou, ov, r.theta, r.gamma, r.p)
+            assert c.value == pytest.approx(otot, rel=1e-9, abs=1e-9), r
+            assert (c.stats["n_approx"], c.stats["n_clamped"]) == (ost["n_approx"], ost["n_clamped"]), r
 
 
 @pytest.mark.gpu

@@ -73,7 +73,16 @@ def _worker(rank, world, port, q, fail_rank):
 
         out = D.sharded_count(len(g["edge_u"]), costs, count_range)
         full = O.exact_count(g["row_ptr"], g["col_idx"], g["edge_u"], g["edge_v"], nthreads=1)
-        q.put((rank, "ok", out["exact"] == full and out["n_exact"] == len(g["edge_u"])))
+        ok = out["exact"] == full and out["n_exact"] == len(g["edge_u"])
+        # the per-step helper bench.py's multi-GPU line uses (strong scaling:
+        # one graph's edges split across the ranks), stepped twice
+        shard = D.ShardedExact(costs, count_range)
+        for _ in range(2):
+            st = shard.step()
+            ok = ok and st["exact"] == full and st["n_exact"] == len(g["edge_u"])
+        bounds = D.shard_bounds(costs, world)
+        ok = ok and (shard.lo, shard.hi) == bounds[rank] and bounds[0][0] == 0 and bounds[-1][1] == len(costs)
+        q.put((rank, "ok", ok))
     except Exception as exc:  # reported to the parent, never hangs
         q.put((rank, "error", type(exc).__name__))
     finally:

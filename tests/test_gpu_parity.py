@@ -94,6 +94,91 @@ def test_rmat_exact_vs_oracle(tchll, oracle, dev, scale):
     assert np.array_equal(_np(pe), pe_ref)
 
 
+def test_rmat22_benched_graph_exact_and_hybrid_vs_oracle(tchll, oracle, dev):
+    """The benched configuration itself: R-MAT scale 22, edge factor 16,
+    (a,b,c) = (0.57,0.19,0.19), seed 1 (64.15 M oriented edges).  Its CSR and
+    exact count are bit-exact against the oracle; at p = 12, theta = gamma =
+    256 the 35 K sketches are bit-exact and the hybrid estimate is within the
+    test tolerance (1e-9 relative; the required bar is 1e-6) of the oracle's
+    FP64 evaluation of the reference estimator (src/hll.py:37-54,
+    src/hybrid.py:95-148), with identical routing stats."""
+    from triangle_counting_hll_b200 import core
+    u, v = core.gen_rmat(22, 16, 0.57, 0.19, 0.19, seed=1, device=dev)
+    g = core.csr_from_edges(u, v)
+    og = _ocsr(oracle, _np(u), _np(v))
+    del u, v
+    _check_csr(g, og)
+    want = oracle.exact_count(og["row_ptr"], og["col_idx"], og["edge_u"], og["edge_v"], nthreads=0)
+    assert _exact(core, g) == want == 2112623785
+    theta, p = 256, 12
+    slot, nr = core.sketch_slots(g.row_ptr, theta)
+    rows = core.build_sketches_compact_tensors(g.row_ptr, g.col_idx, slot, nr, p)
+    oslot, orows = oracle.build_sketches_compact(og["row_ptr"].astype(np.int64), og["col_idx"].astype(np.int64),
+                                                 theta, p)
+    assert np.array_equal(_np(slot), oslot) and np.array_equal(_np(rows), orows)
+    otot, ost, _ = oracle.hybrid_count(og["row_ptr"], og["col_idx"], og["edge_u"], og["edge_v"], og["degrees"],
+                                       oslot, orows, p, theta, nthreads=0)
+    res, _ = core.hybrid_count_compact_tensors(g.row_ptr, g.col_idx, g.edge_u, g.edge_v, g.degrees, rows, slot, p,
+                                               theta, split_kernels=True)
+    tot, r = core.hybrid_from_result(res)
+    assert tot == pytest.approx(otot, rel=HYB_RTOL)
+    assert (int(r.n_approx), int(r.n_exact), int(r.n_fallback), int(r.n_clamped)) == \
+        (ost["n_approx"], ost["n_exact"], ost["n_fallback"], ost["n_clamped"])
+
+
+class _CAIArray:
+    """A foreign device array: only __cuda_array_interface__ and
+    copy_to_host, like a Numba device array (used where Numba's CUDA target
+    cannot start)."""
+
+    def __init__(self, host):
+        import torch
+        self._t = torch.from_numpy(np.ascontiguousarray(host)).cuda()
+        self.__cuda_array_interface__ = self._t.__cuda_array_interface__
+
+    def copy_to_host(self):
+        return self._t.cpu().numpy()
+
+
+def _foreign_to_device():
+    try:
+        from numba import cuda
+        if cuda.is_available():
+            return cuda.to_device, "numba"
+    except Exception:
+        pass
+    return _CAIArray, "cuda_array_interface"
+
+
+def test_numba_device_arrays_at_the_reference_entry_points(tchll, oracle, dev):
+    """The reference's driver hands Numba device arrays (cuda.to_device of
+    the CSR, experiment/exp_gpu.py:686-692) to gpu_exact_triangle_count,
+    build_sketches_kernel[grid, block] and gpu_hybrid_triangle_count: here the
+    same objects go through the package's entry points, the sketch launch
+    writes the registers into the Numba buffers themselves, and every result
+    equals the oracle's."""
+    from triangle_counting_hll_b200 import core
+    to_dev, kind = _foreign_to_device()
+    u, v = core.gen_rmat(14, 16, 0.57, 0.19, 0.19, seed=6, device=dev)
+    g = core.csr_from_edges(u, v)
+    og = _ocsr(oracle, _np(u), _np(v))
+    rp, ci, eu, ev, dg = (to_dev(og[k]) for k in ("row_ptr", "col_idx", "edge_u", "edge_v", "degrees"))
+    want = oracle.exact_count(og["row_ptr"], og["col_idx"], og["edge_u"], og["edge_v"])
+    cnt, elapsed = tchll.gpu_exact_triangle_count(rp, ci, eu, ev)
+    assert cnt == want and elapsed >= 0.0, kind
+    n, p, gamma = g.n_nodes, 10, 32
+    regs = to_dev(np.zeros(n << p, np.uint8))
+    has = to_dev(np.zeros(n, np.uint8))
+    tchll.build_sketches_kernel[(n + 255) // 256, 256](rp, ci, n, gamma, p, regs, has)
+    oregs, ohas = oracle.build_sketches_dense(og["row_ptr"], og["col_idx"], n, gamma, p)
+    assert np.array_equal(has.copy_to_host(), ohas) and np.array_equal(regs.copy_to_host(), oregs), kind
+    otot, ost, _ = oracle.hybrid_count(og["row_ptr"], og["col_idx"], og["edge_u"], og["edge_v"], og["degrees"],
+                                       oracle.dense_slots(ohas), oregs, p, gamma, nthreads=0)
+    est, elapsed, st = tchll.gpu_hybrid_triangle_count(rp, ci, eu, ev, dg, regs, has, gamma, p)
+    assert est == pytest.approx(otot, rel=HYB_RTOL), kind
+    assert (st["n_approx"], st["n_exact"], st["n_clamped"]) == (ost["n_approx"], ost["n_exact"], ost["n_clamped"])
+
+
 def test_c1_c2_configs(tchll, oracle, dev):
     """Erdos-Renyi n=20000 m=100000 seed 0 and the 1000x1000 perturbed lattice."""
     from triangle_counting_hll_b200 import core
@@ -235,6 +320,64 @@ def test_hub_kernel_settings_match_oracle(tchll, oracle, dev):
     with pytest.raises(ValueError):
         core.set_count_tuning(hub=256, hub_seg=100)
     assert core.get_count_tuning()["hub"] == base["hub"]
+
+
+def test_hub_core_bitmap_hash_and_overlap_match_oracle(tchll, oracle, dev):
+    """The hub kernels in core coordinates: the shared-memory bitmap (core
+    fits), hash tables only (bitmap off), a bitmap buffer too small for the
+    core (the bitmap kernel steps aside on the device and the hash kernel
+    counts), each with the hybrid's HLL pass on the side stream or inline:
+    exact counts and hybrid result blocks identical and equal to the oracle."""
+    import torch
+    from triangle_counting_hll_b200 import core
+    u, v = core.gen_rmat(16, 16, 0.57, 0.19, 0.19, seed=11, device=dev)
+    iu, iv = np.triu_indices(600, 1)  # a 600-clique far away in id space: its members join the core
+    u = torch.cat([u, torch.from_numpy((iu * 53 + 70001).astype(np.int32)).to(dev)])
+    v = torch.cat([v, torch.from_numpy((iv * 53 + 70001).astype(np.int32)).to(dev)])
+    g = core.csr_from_edges(u, v)
+    og = _ocsr(oracle, _np(u), _np(v))
+    want = oracle.exact_count(og["row_ptr"], og["col_idx"], og["edge_u"], og["edge_v"], nthreads=0)
+    theta, p = 96, 10
+    slot, nr = core.sketch_slots(g.row_ptr, theta)
+    rows = core.build_sketches_compact_tensors(g.row_ptr, g.col_idx, slot, nr, p)
+    oslot, orows = oracle.build_sketches_compact(og["row_ptr"].astype(np.int64), og["col_idx"].astype(np.int64),
+                                                 theta, p)
+    otot, ost, _ = oracle.hybrid_count(og["row_ptr"], og["col_idx"], og["edge_u"], og["edge_v"], og["degrees"],
+                                       oslot, orows, p, theta, nthreads=0)
+    base = core.get_count_tuning()
+    blocks = []
+    try:
+        for hub, blg, ov in ((128, 15, 1), (128, 0, 1), (64, 10, 0), (64, 15, 0), (128, 12, 1), (200, 17, 1)):
+            core.set_count_tuning(base["chunk"], base["slots_log2"], base["tiny"], base["blocks_per_sm"], hub=hub,
+                                  bitmap_lg=blg, overlap=bool(ov))
+            assert core.get_count_tuning()["bitmap_lg"] == blg
+            assert _exact(core, g) == want, (hub, blg, ov)
+            res, _ = core.hybrid_count_compact_tensors(g.row_ptr, g.col_idx, g.edge_u, g.edge_v, g.degrees, rows,
+                                                       slot, p, theta, split_kernels=True)
+            tot, r = core.hybrid_from_result(res)
+            assert tot == pytest.approx(otot, rel=HYB_RTOL), (hub, blg, ov)
+            assert (int(r.n_approx), int(r.n_exact), int(r.n_clamped)) == \
+                (ost["n_approx"], ost["n_exact"], ost["n_clamped"])
+            blocks.append(bytes(_np(res)))
+    finally:
+        core.set_count_tuning(**base)
+    assert all(b == blocks[0] for b in blocks)  # fixed-point totals: byte-identical blocks
+    with pytest.raises(ValueError):
+        core.set_count_tuning(bitmap_lg=9)
+
+
+def test_hub_path_rejects_out_of_range_neighbour_ids(tchll, dev):
+    """The hub kernels read col_idx values as vertex indices: a value outside
+    [0, n_nodes) in a hub list is reported (ValueError), never dereferenced."""
+    from triangle_counting_hll_b200 import core
+    iu, iv = np.triu_indices(300, 1)  # forward lists up to 299 long: the hub path runs
+    g = core.csr_from_edges(iu.astype(np.int32), iv.astype(np.int32), device=dev)
+    assert _exact(core, g) == 300 * 299 * 298 // 6
+    col = g.col_idx.clone()
+    col[5] = g.n_nodes + 1000
+    with pytest.raises(ValueError, match="neighbour id"):
+        res, _ = core.exact_count_tensors(g.row_ptr, col, g.edge_u, g.edge_v)
+        core.exact_from_result(res)
 
 
 # ---------------------------------------------------------------- sketches
@@ -433,6 +576,45 @@ def test_hybrid_zero_masks_give_identical_results(tchll, oracle, dev, p):
                                        oracle.dense_slots(ohas), oregs, p, theta, nthreads=0)
     assert int(r.n_approx) == ost["n_approx"] > 0 and int(r.n_clamped) == ost["n_clamped"]
     assert tot == pytest.approx(otot, rel=HYB_RTOL)
+
+
+@pytest.mark.parametrize("p", [4, 8, 10, 12, 16])
+def test_hll_pass_settings_give_identical_results(tchll, oracle, dev, p):
+    """The HLL pass as one pass over both register rows (byte-permute table
+    for ranks <= 7, exact 64-bit sums above) and as zero masks first, at
+    every group width: byte-identical result blocks, equal to the oracle.
+    Includes rows with high ranks (a 5000-clique's hub sketches) so the
+    byte-by-byte branch runs."""
+    import torch
+    from triangle_counting_hll_b200 import core
+    u, v = core.gen_rmat(14, 16, 0.57, 0.19, 0.19, seed=13, device=dev)
+    iu, iv = np.triu_indices(2000, 1)
+    u = torch.cat([u, torch.from_numpy((iu * 3 + 5).astype(np.int32)).to(dev)])
+    v = torch.cat([v, torch.from_numpy((iv * 3 + 5).astype(np.int32)).to(dev)])
+    g = core.csr_from_edges(u, v)
+    theta = 24
+    slot, nr = core.sketch_slots(g.row_ptr, theta)
+    rows = core.build_sketches_compact_tensors(g.row_ptr, g.col_idx, slot, nr, p)
+    assert int(rows.max()) >= 8  # ranks above the table path occur
+    og = _ocsr(oracle, _np(u), _np(v))
+    oslot, orows = oracle.build_sketches_compact(og["row_ptr"].astype(np.int64), og["col_idx"].astype(np.int64),
+                                                 theta, p)
+    otot, ost, _ = oracle.hybrid_count(og["row_ptr"], og["col_idx"], og["edge_u"], og["edge_v"], og["degrees"],
+                                       oslot, orows, p, theta, nthreads=0)
+    base = core.get_count_tuning()
+    blocks = []
+    try:
+        for onepass_p, lanes in ((10, 0), (16, 0), (0, 0), (16, 1), (16, 4), (16, 32), (0, 2), (0, 32)):
+            core.set_count_tuning(**{**base, "hll_onepass_p": onepass_p, "hll_lanes": lanes})
+            res, _ = core.hybrid_count_compact_tensors(g.row_ptr, g.col_idx, g.edge_u, g.edge_v, g.degrees, rows,
+                                                       slot, p, theta, split_kernels=True)
+            tot, r = core.hybrid_from_result(res)
+            assert tot == pytest.approx(otot, rel=HYB_RTOL), (onepass_p, lanes)
+            assert (int(r.n_approx), int(r.n_clamped)) == (ost["n_approx"], ost["n_clamped"]), (onepass_p, lanes)
+            blocks.append(bytes(_np(res)))
+    finally:
+        core.set_count_tuning(**base)
+    assert ost["n_approx"] > 0 and all(b == blocks[0] for b in blocks)
 
 
 def test_hybrid_all_exact_equals_exact(tchll, dev):

@@ -41,7 +41,7 @@ def _noalloc_count(L, g, torch, dev, stream):
     return rc, res
 
 
-def test_noalloc_matches_workspace_entry_point(tchll):
+def test_noalloc_matches_workspace_entry_point(tchll, oracle):
     import torch
 
     from triangle_counting_hll_b200 import _lib, core
@@ -54,6 +54,10 @@ def test_noalloc_matches_workspace_entry_point(tchll):
         g = core.csr_from_edges(u, v)
         ref = _lib.read_count_result(_workspace_count(L, g, torch, dev, stream))
         assert ref.status == 0 and ref.exact > 0
+        # and independently of the shared counting code: the CPU oracle on
+        # its own CSR of the same edge list
+        og = oracle.csr_build(u.cpu().numpy(), v.cpu().numpy())
+        assert ref.exact == oracle.exact_count(og["row_ptr"], og["col_idx"], og["edge_u"], og["edge_v"], nthreads=0)
         for _ in range(2):  # two calls in a row share the fixed scratch
             rc, res = _noalloc_count(L, g, torch, dev, stream)
             assert rc == 0, _lib.last_error()

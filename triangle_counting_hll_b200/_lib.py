@@ -29,6 +29,7 @@ TCHLL_EWORKSPACE = 3
 STATUS_BAD_EDGE = 1
 STATUS_BAD_ROW = 2
 STATUS_BAD_SLOT = 4
+STATUS_BAD_KEY = 8
 
 
 class TchllError(RuntimeError):
@@ -71,6 +72,10 @@ SIGNATURES = {
     "tchll_get_count_tuning": (C.c_int, [_P]),
     "tchll_set_count_hub": (C.c_int, [_I32, _I32, _I32, _I32]),
     "tchll_get_count_hub": (C.c_int, [_P]),
+    "tchll_set_count_core": (C.c_int, [_I32, _I32]),
+    "tchll_get_count_core": (C.c_int, [_P]),
+    "tchll_set_hll_pass": (C.c_int, [_I32, _I32]),
+    "tchll_get_hll_pass": (C.c_int, [_P]),
     "tchll_exact_count_noalloc": (C.c_int, [_P, _I64, _P, _I64, _P, _P, _I64, _P, _P]),
     "tchll_set_phase_timing": (C.c_int, [_I32]),
     "tchll_phase_times": (C.c_int, [_P]),
@@ -248,6 +253,8 @@ def raise_on_status(res: CountResult) -> None:
             parts.append("row_ptr extent outside [0, nnz] or decreasing")
         if res.status & STATUS_BAD_SLOT:
             parts.append("sketch slot outside the register rows")
+        if res.status & STATUS_BAD_KEY:
+            parts.append("neighbour id outside [0, n_nodes)")
         raise ValueError("malformed graph input: " + "; ".join(parts))
 
 

@@ -249,13 +249,22 @@ def hybrid_count_compact_tensors(row_ptr, col_idx, edge_u, edge_v, degrees, rows
 def set_count_tuning(chunk: int = 256, slots_log2: int = 11, tiny: int = 16, blocks_per_sm: int = 0,
                      warps: Optional[int] = None, pairs: Optional[bool] = None,
                      sparse: Optional[bool] = None, hub: Optional[int] = None, hub_seg: Optional[int] = None,
-                     hub_lg: Optional[int] = None, hub_unroll: Optional[int] = None) -> None:
+                     hub_lg: Optional[int] = None, hub_unroll: Optional[int] = None,
+                     bitmap_lg: Optional[int] = None, overlap: Optional[bool] = None,
+                     hll_onepass_p: Optional[int] = None, hll_lanes: Optional[int] = None) -> None:
     """Launch shape of the counting kernels (results do not depend on it).
     hub / hub_seg / hub_lg / hub_unroll: threshold on d+(x) above which a pair
-    goes to the CTA-shared table kernel (0: off), pairs per work unit, log2
-    table slots, probe loads in flight per lane."""
+    goes to the CTA-shared table kernels (0: off), pairs per work unit, log2
+    hash-table slots, probe loads in flight per lane.  bitmap_lg: log2 bytes
+    of the hub bitmap buffer (0: hash tables only); overlap: hybrid HLL pass
+    on a second stream beside the exact pairs.  hll_onepass_p / hll_lanes:
+    the HLL pass's one-pass threshold on p and lanes per edge (0: by p)."""
     L = load()
     cur = get_count_tuning()
+    check(L.tchll_set_hll_pass(int(cur["hll_onepass_p"] if hll_onepass_p is None else hll_onepass_p),
+                               int(cur["hll_lanes"] if hll_lanes is None else hll_lanes)))
+    check(L.tchll_set_count_core(int(cur["bitmap_lg"] if bitmap_lg is None else bitmap_lg),
+                                 int(cur["overlap"] if overlap is None else bool(overlap))))
     check(L.tchll_set_count_hub(int(cur["hub"] if hub is None else hub),
                                 int(cur["hub_seg"] if hub_seg is None else hub_seg),
                                 int(cur["hub_lg"] if hub_lg is None else hub_lg),
@@ -274,9 +283,14 @@ def get_count_tuning() -> dict:
     check(load().tchll_get_count_tuning(C.cast(out, C.c_void_p)))
     hub = (C.c_int32 * 4)()
     check(load().tchll_get_count_hub(C.cast(hub, C.c_void_p)))
+    co = (C.c_int32 * 2)()
+    check(load().tchll_get_count_core(C.cast(co, C.c_void_p)))
+    hp = (C.c_int32 * 2)()
+    check(load().tchll_get_hll_pass(C.cast(hp, C.c_void_p)))
     return {"chunk": out[0], "slots_log2": out[1], "tiny": out[2], "blocks_per_sm": out[3], "warps": out[4],
             "pairs": out[5], "sparse": out[6], "hub": hub[0], "hub_seg": hub[1], "hub_lg": hub[2],
-            "hub_unroll": hub[3]}
+            "hub_unroll": hub[3], "bitmap_lg": co[0], "overlap": co[1], "hll_onepass_p": hp[0],
+            "hll_lanes": hp[1]}
 
 
 def set_phase_timing(enable: bool) -> None:
@@ -290,9 +304,10 @@ def phase_times() -> dict:
     check(load().tchll_phase_times(C.cast(out, C.c_void_p)))
     names = ("pairs", "count", "hll")
     res = {n: (float(v) if v >= 0 else None) for n, v in zip(names, out)}
-    hub = C.c_float(-1.0)
-    check(load().tchll_phase_hub_ms(C.byref(hub)))
-    res["hub"] = float(hub.value) if hub.value >= 0 else None  # part of "count"
+    hub = (C.c_float * 2)()
+    check(load().tchll_phase_hub_ms(C.cast(hub, C.c_void_p)))
+    res["hub"] = float(hub[0]) if hub[0] >= 0 else None        # hub kernels, part of "count"
+    res["hub_core"] = float(hub[1]) if hub[1] >= 0 else None   # core pass before them, part of "count"
     return res
 
 

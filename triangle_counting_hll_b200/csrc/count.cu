@@ -42,6 +42,7 @@
 //     on scheduling or partitioning: they are bit-identical run to run.
 #include <cub/cub.cuh>
 
+#include <atomic>
 #include <mutex>
 
 #include "common.cuh"
@@ -55,6 +56,7 @@ enum : uint32_t {
     ST_BAD_EDGE = 1u,  // edge endpoint outside [0, n_nodes)
     ST_BAD_ROW = 2u,   // row_ptr extent outside [0, nnz] or decreasing
     ST_BAD_SLOT = 4u,  // sketch slot outside [0, n_rows)
+    ST_BAD_KEY = 8u,   // neighbour id (col_idx value) outside [0, n_nodes)
 };
 
 struct CountParams {
@@ -698,49 +700,131 @@ struct HubSeg {
 
 struct HubParams {
     const int32_t* row_ptr;
+    int64_t n_nodes;
     const int32_t* col_idx;
     int64_t nnz;
     const int32_t* hy;  // y of each hub pair, grouped by x
-    const int32_t* pcol;  // padded lists (pad_rows_kernel) or null
+    const int32_t* pcol;  // core-filtered padded lists (core_pad_kernel) or null: raw lists
+    const int32_t* cidx;  // core index of each vertex, -1 outside the core (with pcol)
+    const int32_t* plen;  // filtered length of each probe list (with pcol)
+    const int32_t* n_core;  // device scalar: core size C (with pcol)
     const HubSeg* segs;
     const unsigned long long* n_segs;
     int64_t max_segs;
     unsigned long long* seg_ctr;
-    int hub_lg;    // log2 of the largest table (slots)
+    int hub_lg;    // log2 of the largest hash table (slots)
+    int cap_bits;  // bitmap kernel: bits its shared buffer holds
     bool batched;  // publish per segment into result[segment graph]
     tchll_count_result* result;
 };
 
-// Padded probe lists: row y's list starts at element pad_start(y), a multiple
-// of 4, and is followed by OV_NONE up to the next multiple of 4, so every
-// 16-byte quad holds only the list's keys or OV_NONE and no probe needs a
-// mask.  pad_start(y) = roundup4(row_ptr[y]) + 8 y leaves room for the
-// padding of every row before y (at most 3 per row) without a scan.
+// The hub core.  Every key that can match a hub table lies in the forward
+// list of some table side x that has hub pairs; call the union of those
+// lists the core (R-MAT scale 22: 108 K of 2.4 M vertices, because
+// orientation by (degree, id) puts every long list's members among the
+// highest-degree vertices).  The hub kernels work in core coordinates:
+//   * cidx[w] = rank of w among the core vertices (ascending id), else -1;
+//   * each probe list is rewritten as the core indices of its members only
+//     (keys outside the core can never hit, 31% of the hub probes on R-MAT
+//     scale 22), padded with the never-set sentinel C (the core size);
+//   * a table side's list becomes a C-bit bitmap in shared memory (13.5 KB
+//     on R-MAT scale 22), so a probe is one shift, one 4-byte shared load
+//     and one funnel shift.
+// Counts are unchanged: |N+(x) cap N+(y)| = |cidx(N+(x)) cap cidx(N+(y) cap
+// core)| because N+(x) lies inside the core and cidx is one-to-one there.
+//
+// Padded probe lists: row y's list starts at element pad_start(y), a
+// multiple of 4, and is followed by the sentinel up to the next multiple of
+// 4, so every 16-byte quad holds only the list's keys or the sentinel and no
+// probe needs a mask.  pad_start(y) = roundup4(row_ptr[y]) + 8 y leaves room
+// for the padding of every row before y (at most 3 per row) without a scan.
 __device__ __forceinline__ int64_t pad_start(int32_t rs, int32_t y) {
     return (((int64_t)rs + 3) & ~(int64_t)3) + 8 * (int64_t)y;
 }
 
-__global__ void pad_rows_kernel(const int32_t* __restrict__ row_ptr, int64_t n_nodes,
-                                const int32_t* __restrict__ col, int32_t* __restrict__ pcol) {
-    const int sub = threadIdx.x & 7;  // 8 lanes per row, one 16-byte quad each
-    const int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 3;
-    const int64_t ng = ((int64_t)gridDim.x * blockDim.x) >> 3;
-    for (int64_t y = g; y < n_nodes; y += ng) {
-        const int32_t rs = __ldg(row_ptr + y);
-        const int32_t d = __ldg(row_ptr + y + 1) - rs;
-        if (d <= 0) continue;
-        const int64_t ps = pad_start(rs, (int32_t)y);  // a multiple of 4: 16-byte aligned stores
-        const int32_t nq = (d + 3) >> 2;
-        for (int32_t q = sub; q < nq; q += 8) {
-            const int32_t i = 4 * q;
-            int4 w;
-            w.x = __ldg(col + rs + i);  // i < d
-            w.y = i + 1 < d ? __ldg(col + rs + i + 1) : (int32_t)OV_NONE;
-            w.z = i + 2 < d ? __ldg(col + rs + i + 2) : (int32_t)OV_NONE;
-            w.w = i + 3 < d ? __ldg(col + rs + i + 3) : (int32_t)OV_NONE;
-            *reinterpret_cast<int4*>(pcol + ps + i) = w;
+// flag[w] = 1 for every w in N+(x) of every x with hub pairs (cnth[x] > 0).
+// One warp per 32 consecutive x; the warp stores the flags of each hub x's
+// list together.  Values outside [0, n_nodes) are reported, not stored.
+__global__ void core_mark_kernel(const int32_t* __restrict__ row_ptr, int64_t n_nodes, int64_t nnz,
+                                 const int32_t* __restrict__ col, const int32_t* __restrict__ cnth, int32_t* flag,
+                                 tchll_count_result* result) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    uint32_t status = 0;
+    for (int64_t x0 = warp * 32; x0 < n_nodes; x0 += nwarps * 32) {
+        const int64_t x = x0 + lane;
+        const bool hub = x < n_nodes && __ldg(cnth + x) > 0;
+        unsigned b = __ballot_sync(FULL, hub);
+        while (b) {
+            const int j = __ffs(b) - 1;
+            b &= b - 1;
+            const int32_t s = __ldg(row_ptr + x0 + j), e = __ldg(row_ptr + x0 + j + 1);
+            if (s < 0 || e < s || (int64_t)e > nnz) {  // warp-uniform
+                status |= ST_BAD_ROW;
+                continue;
+            }
+            for (int32_t i = s + lane; i < e; i += 32) {
+                const int32_t w = __ldg(col + i);
+                if ((uint64_t)(uint32_t)w < (uint64_t)n_nodes) flag[w] = 1;
+                else status |= ST_BAD_KEY;
+            }
         }
     }
+    status = __reduce_or_sync(FULL, status);
+    if (lane == 0 && status) atomicOr(&result->status, status);
+}
+
+// After the exclusive scan pos = scan(flag) over n_nodes + 1 entries (flag[n]
+// = 0): cidx[w] = pos[w] for flagged w, else -1 (written over flag), and
+// *n_core = pos[n_nodes].
+__global__ void core_index_kernel(int32_t* flag_cidx, const int32_t* __restrict__ pos, int64_t n_nodes,
+                                  int32_t* n_core) {
+    for (int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; w <= n_nodes;
+         w += (int64_t)gridDim.x * blockDim.x) {
+        if (w == n_nodes) *n_core = __ldg(pos + n_nodes);
+        else flag_cidx[w] = flag_cidx[w] ? __ldg(pos + w) : -1;
+    }
+}
+
+// Core-filtered padded probe lists, one warp per row: the core indices of
+// N+(y)'s core members in list order, then the sentinel C up to a multiple
+// of 4; plen[y] = number of core members.  Malformed rows get length 0 and a
+// status flag (the counting kernels flag them too when an edge uses them).
+__global__ void core_pad_kernel(const int32_t* __restrict__ row_ptr, int64_t n_nodes, int64_t nnz,
+                                const int32_t* __restrict__ col, const int32_t* __restrict__ cidx,
+                                const int32_t* __restrict__ n_core, int32_t* __restrict__ pcol,
+                                int32_t* __restrict__ plen, tchll_count_result* result) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int32_t C = *n_core;
+    uint32_t status = 0;
+    for (int64_t y = warp; y < n_nodes; y += nwarps) {
+        const int32_t rs = __ldg(row_ptr + y), re = __ldg(row_ptr + y + 1);
+        int32_t len = 0;
+        if (rs < 0 || re < rs || (int64_t)re > nnz) {
+            status |= ST_BAD_ROW;
+        } else {
+            const int64_t ps = pad_start(rs, (int32_t)y);
+            for (int32_t i0 = rs; i0 < re; i0 += 32) {  // warp-uniform
+                int32_t c = -1;
+                if (i0 + lane < re) {
+                    const int32_t w = __ldg(col + i0 + lane);
+                    if ((uint64_t)(uint32_t)w < (uint64_t)n_nodes) c = __ldg(cidx + w);
+                    else status |= ST_BAD_KEY;
+                }
+                const unsigned bal = __ballot_sync(FULL, c >= 0);
+                if (c >= 0) pcol[ps + len + __popc(bal & lt)] = c;
+                len += __popc(bal);
+            }
+            if (lane < ((-len) & 3)) pcol[ps + len + lane] = C;
+        }
+        if (lane == 0) plen[y] = len;
+    }
+    status = __reduce_or_sync(FULL, status);
+    if (lane == 0 && status) atomicOr(&result->status, status);
 }
 
 template <int UNR, bool PAD>
@@ -749,6 +833,7 @@ __global__ void __launch_bounds__(256, 5) hub_count_kernel(const HubParams H) {
     __shared__ HubSeg s_seg;
     __shared__ int s_round;
     __shared__ int s_fail;
+    if (PAD && H.cap_bits > 0 && *H.n_core + 32 <= H.cap_bits) return;  // the bitmap kernel counted every segment
     const int tid = threadIdx.x, lane = tid & 31;
     const int32_t* __restrict__ col = H.col_idx;
     const int64_t nseg = min((int64_t)*H.n_segs, H.max_segs);
@@ -782,8 +867,17 @@ __global__ void __launch_bounds__(256, 5) hub_count_kernel(const HubParams H) {
             for (int i = tid; i < (1 << lgs) / 4; i += blockDim.x)
                 reinterpret_cast<uint4*>(tbl)[i] = make_uint4(OV_KEY, OV_KEY, OV_KEY, OV_KEY);
             __syncthreads();
-            for (int i = tid; i < xl; i += blockDim.x)
-                if (!ov_insert(tbl, __ldg(col + xs + i), sh, mask)) s_fail = 1;
+            for (int i = tid; i < xl; i += blockDim.x) {
+                int32_t key = __ldg(col + xs + i);
+                if (PAD) {  // core coordinates: every member of a hub list is in the core
+                    key = (uint64_t)(uint32_t)key < (uint64_t)H.n_nodes ? __ldg(H.cidx + key) : -1;
+                    if (key < 0) {
+                        s_fail = 1;
+                        continue;
+                    }
+                }
+                if (!ov_insert(tbl, key, sh, mask)) s_fail = 1;
+            }
             __syncthreads();
         }
         const bool table = fits && !s_fail;  // CTA-uniform
@@ -804,7 +898,7 @@ __global__ void __launch_bounds__(256, 5) hub_count_kernel(const HubParams H) {
                 re = __ldg(H.row_ptr + y + 1);
                 if (PAD) {
                     vs = (int32_t)pad_start(rs, y);
-                    ve = vs + ((re - rs + 3) & ~3);
+                    ve = vs + ((__ldg(H.plen + y) + 3) & ~3);
                 } else {
                     vs = rs;
                     ve = re;
@@ -838,6 +932,10 @@ __global__ void __launch_bounds__(256, 5) hub_count_kernel(const HubParams H) {
             const int excl = incl - c_nq;
             const int W = __shfl_sync(FULL, incl, 31);
             const int qb = c_q0 - excl;
+            // a lane's list: starts before its window + starts in the window
+            // up to the lane - 1 (B: the window's list starts)
+            const unsigned lane_le = (2u << lane) - 1u;
+            int S = 0;
             for (int T0 = 0; T0 < W; T0 += 32 * UNR) {
                 int qd[UNR], lo[UNR], hi[UNR];
 #pragma unroll
@@ -846,11 +944,10 @@ __global__ void __launch_bounds__(256, 5) hub_count_kernel(const HubParams H) {
                     qd[i] = -1;
                     lo[i] = hi[i] = 0;
                     if (Ti < W) {  // warp-uniform
-                        const unsigned cover = __ballot_sync(FULL, lane < k && excl <= Ti && Ti < incl);
-                        const int b = __ffs(cover) - 1;
-                        const unsigned bit = (lane < k && excl > Ti && excl < Ti + 32) ? (1u << (excl - Ti)) : 0u;
-                        const unsigned B = __reduce_or_sync(FULL, bit);
-                        const int j = (b + __popc(B & ((2u << lane) - 1u))) & 31;
+                        const unsigned d = (unsigned)(excl - Ti);
+                        const unsigned B = __reduce_or_sync(FULL, (lane < k && d < 32u) ? (1u << d) : 0u);
+                        const int j = (S + __popc(B & lane_le) - 1) & 31;
+                        S += __popc(B);
                         const int my_qb = __shfl_sync(FULL, qb, j);
                         const int32_t my_vs = __shfl_sync(FULL, c_vs, j);
                         const int32_t my_ve = __shfl_sync(FULL, c_ve, j);
@@ -934,6 +1031,163 @@ __global__ void __launch_bounds__(256, 5) hub_count_kernel(const HubParams H) {
             n_pairs = 0;
         }
         __syncthreads();  // every warp is done with this table
+    }
+    if (H.batched) return;
+    acc = warp_sum_u64(acc);
+    n_pairs = warp_sum_i64(n_pairs);
+    if (lane == 0) {
+        if (acc) atomicAdd((unsigned long long*)&H.result->exact, (unsigned long long)acc);
+        if (n_pairs) atomicAdd((unsigned long long*)&H.result->n_exact, (unsigned long long)n_pairs);
+    }
+}
+
+// Hub pairs over a shared-memory bitmap of N+(x) in core coordinates (see
+// the hub core above).  Runs only when the core fits the shared buffer
+// (C + 32 <= cap_bits, decided on the device: the host never reads C);
+// otherwise it returns at once and hub_count_kernel<*, true> takes the
+// segments from the same counter.
+//
+// A CTA claims a segment, clears ceil((C + 32) / 128) uint4 words, sets the
+// bits of x's list and its warps stream the segment's probe lists through
+// it, up to 32 lists per round.  The round's lists are flattened into one
+// stream of 16-byte quads, 32 consecutive quads per window dealt to the 32
+// lanes (coalesced loads).  A lane finds its quad's list from the bitmap B
+// of list starts inside its window (one OR-reduction per window): list index
+// = starts before the window + starts up to the lane - 1.  Since the probe
+// lists are core-filtered and padded with the never-set bit C, a key needs no
+// mask and no bound: hit = bit key of the bitmap.
+template <int UNR>
+__global__ void __launch_bounds__(256, 6) hub_bitmap_kernel(const HubParams H) {
+    extern __shared__ __align__(16) uint32_t bm[];
+    __shared__ HubSeg s_seg;
+    __shared__ int s_round;
+    __shared__ int s_fail;
+    const int C = *H.n_core;
+    if (C + 32 > H.cap_bits) return;  // grid-uniform: the hash kernel takes over
+    const int tid = threadIdx.x, lane = tid & 31;
+    const unsigned lane_le = (2u << lane) - 1u;  // lane 31: 0 - 1 = all bits
+    const uint32_t sentinel = (uint32_t)C;
+    const int nw4 = (C + 32 + 127) >> 7;  // uint4 words covering bits [0, C + 32)
+    const int32_t* __restrict__ col = H.col_idx;
+    const uint4* __restrict__ pq = reinterpret_cast<const uint4*>(H.pcol);
+    const int64_t nseg = min((int64_t)*H.n_segs, H.max_segs);
+    uint64_t acc = 0;
+    int64_t n_pairs = 0;
+    while (true) {
+        if (tid == 0) {
+            const unsigned long long s = atomicAdd(H.seg_ctr, 1ull);
+            if ((int64_t)s < nseg) {
+                s_seg = H.segs[s];
+            } else {
+                s_seg.x = -1;
+                s_seg.len = 0;
+                s_seg.start = 0;
+            }
+            s_round = 0;
+            s_fail = 0;
+        }
+        for (int i = tid; i < nw4; i += blockDim.x) reinterpret_cast<uint4*>(bm)[i] = make_uint4(0u, 0u, 0u, 0u);
+        __syncthreads();
+        const HubSeg sg = s_seg;
+        if (sg.x < 0) break;
+        if (tid == 0) n_pairs += sg.len;
+        const int32_t xs = __ldg(H.row_ptr + sg.x);
+        const int xl = __ldg(H.row_ptr + sg.x + 1) - xs;
+        for (int i = tid; i < xl; i += blockDim.x) {
+            const int32_t w = __ldg(col + xs + i);
+            const int32_t c = (uint64_t)(uint32_t)w < (uint64_t)H.n_nodes ? __ldg(H.cidx + w) : -1;
+            if (c >= 0) atomicOr(bm + (c >> 5), 1u << (c & 31));
+            else s_fail = 1;  // not in the core (cannot happen for well-formed input)
+        }
+        __syncthreads();
+        const bool table = !s_fail;  // CTA-uniform
+        // pairs per round: up to 32, fewer for short segments so that every
+        // warp of the CTA gets about two rounds
+        int rsz = (sg.len + 15) >> 4;
+        rsz = rsz < 4 ? 4 : (rsz > 32 ? 32 : rsz);
+        while (true) {
+            int r = 0;
+            if (lane == 0) r = atomicAdd(&s_round, rsz);
+            r = __shfl_sync(FULL, r, 0);
+            if (r >= sg.len) break;
+            const int np = min(rsz, sg.len - r);
+            int32_t vs = 0, nq = 0, rs = 0, re = 0;
+            if (lane < np) {
+                const int32_t y = __ldg(H.hy + sg.start + r + lane);
+                rs = __ldg(H.row_ptr + y);
+                if (table) {
+                    vs = (int32_t)pad_start(rs, y);
+                    nq = (__ldg(H.plen + y) + 3) >> 2;
+                } else {
+                    re = __ldg(H.row_ptr + y + 1);
+                }
+            }
+            if (!table) {  // binary search per pair over the raw lists
+                for (int j = 0; j < np; ++j) {
+                    const int32_t jrs = __shfl_sync(FULL, rs, j);
+                    const int32_t jre = __shfl_sync(FULL, re, j);
+                    acc += warp_bsearch_count(col + xs, xl, col + jrs, jre - jrs, lane);
+                }
+                continue;
+            }
+            // the round's non-empty lists, compacted to lanes 0..k-1, and the
+            // exclusive scan of their quad counts
+            const unsigned ne = __ballot_sync(FULL, nq > 0);
+            const int k = __popc(ne);
+            const int src = lane < k ? (int)__fns(ne, 0, lane + 1) : lane;
+            const int c_q0 = __shfl_sync(FULL, vs >> 2, src);
+            int c_nq = __shfl_sync(FULL, nq, src);
+            if (lane >= k) c_nq = 0;
+            int incl = c_nq;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += t;
+            }
+            const int excl = incl - c_nq;
+            const int W = __shfl_sync(FULL, incl, 31);
+            const int qb = c_q0 - excl;  // quad of stream position t in list j: qb[j] + t
+            const bool starts = lane < k;
+            int S = 0;  // list starts before the current window
+            for (int T0 = 0; T0 < W; T0 += 32 * UNR) {
+                int qd[UNR];
+#pragma unroll
+                for (int i = 0; i < UNR; ++i) {
+                    const int Ti = T0 + 32 * i;
+                    qd[i] = -1;
+                    if (Ti < W) {  // warp-uniform
+                        const unsigned d = (unsigned)(excl - Ti);
+                        const unsigned B = __reduce_or_sync(FULL, (starts && d < 32u) ? (1u << d) : 0u);
+                        const int j = S + __popc(B & lane_le) - 1;
+                        S += __popc(B);
+                        const int my_qb = __shfl_sync(FULL, qb, j & 31);
+                        if (Ti + lane < W) qd[i] = my_qb + Ti + lane;
+                    }
+                }
+                uint32_t key[4 * UNR];
+#pragma unroll
+                for (int i = 0; i < UNR; ++i) {
+                    uint4 q = make_uint4(sentinel, sentinel, sentinel, sentinel);
+                    if (qd[i] >= 0) q = __ldg(pq + qd[i]);
+                    key[4 * i + 0] = q.x;
+                    key[4 * i + 1] = q.y;
+                    key[4 * i + 2] = q.z;
+                    key[4 * i + 3] = q.w;
+                }
+                uint32_t c = 0;
+#pragma unroll
+                for (int t = 0; t < 4 * UNR; ++t) c += __funnelshift_r(bm[key[t] >> 5], 0u, key[t]) & 1u;
+                acc += c;
+            }
+        }
+        if (H.batched) {  // this segment's totals belong to its graph
+            acc = warp_sum_u64(acc);
+            if (lane == 0 && acc) atomicAdd((unsigned long long*)&H.result[sg.graph].exact, (unsigned long long)acc);
+            if (tid == 0) atomicAdd((unsigned long long*)&H.result[sg.graph].n_exact, (unsigned long long)sg.len);
+            acc = 0;
+            n_pairs = 0;
+        }
+        __syncthreads();  // every warp is done with this bitmap
     }
     if (H.batched) return;
     acc = warp_sum_u64(acc);
@@ -1074,19 +1328,89 @@ __device__ __forceinline__ U128 group_sum_u128(U128 v, unsigned gmask) {
     return v;
 }
 
-__device__ __forceinline__ void hll_word128(uint32_t w, int S, U128& sum, double& extra) {
-    if (w == 0u) return;
+// Sum of 2^-r over the merged registers, exactly, in units of 2^-S
+// (S = 65 - p, so 2^-r for every valid rank r <= S is an integer there).
+// Most registers hold r <= 7: for a word w of four such registers,
+//   t    = bytes 2^(7 - r_i)   (one byte permute of the table 128, 64 .. 1,
+//                               selected by the four ranks packed as nibbles)
+//   fast += bytes of t          (dp4a with 1,1,1,1)
+//   zeros += [r_i == 0]         (a second permute of the table 1,0,..,0)
+// so fast * 2^(S-7) is the words' share of the sum.  A word with a register
+// >= 8 goes byte by byte: r <= 7 into fast, 8 <= r <= S into fine (units of
+// 2^-S, 64 bits), r > S (only in malformed rows) into extra (FP64).
+__device__ __forceinline__ void hll_word_lut(uint32_t w, int S, uint32_t& fast, uint64_t& fine, uint32_t& zeros,
+                                             double& extra) {
+    if ((w & 0xF8F8F8F8u) == 0u) {
+        const uint32_t x = w | (w >> 4);                 // byte 0: r0 | r1 << 4, byte 2: r2 | r3 << 4
+        const uint32_t sel = __byte_perm(x, 0u, 0x4420u);  // nibbles r0 r1 r2 r3
+        fast = __dp4a(__byte_perm(0x10204080u, 0x01020408u, sel), 0x01010101u, fast);
+        zeros = __dp4a(__byte_perm(0x00000001u, 0u, sel), 0x01010101u, zeros);
+        return;
+    }
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        const uint32_t r = (w >> (8 * k)) & 0xFFu;
-        if (r != 0u) {
-            if ((int)r <= S) sum.add(1ull << (S - (int)r));
-            else extra += ldexp(1.0, S - (int)r);
+        const int r = (int)((w >> (8 * k)) & 0xFFu);
+        if (r <= 7) {
+            fast += 128u >> r;
+            zeros += (r == 0);
+        } else if (r <= S) {
+            fine += 1ull << (S - r);
+        } else {
+            extra += ldexp(1.0, S - r);
         }
     }
 }
 
-template <int L, bool ZM, bool CACHE>
+template <int L>
+__device__ __forceinline__ uint64_t group_sum_u64(uint64_t x, unsigned gmask) {
+#pragma unroll
+    for (int o = L / 2; o > 0; o >>= 1) x += __shfl_xor_sync(gmask, x, o);
+    return x;
+}
+
+// E = the reference's estimate of the merged row from Z = ldexp(zsum, -S)
+// (zsum exact, plus extra) and the zero count V (src/hll.py:37-54; variant 1:
+// cpu_exp's 2^32 correction, cpu_exp/triangle_hll_experiment.py:357-366).
+__device__ __forceinline__ double hll_estimate_from(U128 zsum, double extra, uint32_t zeros, int p, int S,
+                                                    int variant) {
+    const int m = 1 << p;
+    const double Z = ldexp(u128_to_double(zsum.lo, zsum.hi) + extra, -S);
+    double alpha;
+    if (m == 16) alpha = 0.673;
+    else if (m == 32) alpha = 0.697;
+    else if (m == 64) alpha = 0.709;
+    else alpha = 0.7213 / (1.0 + 1.079 / (double)m);
+    double E = alpha * (double)m * (double)m / Z;
+    if (variant == 1) {
+        if (E <= 2.5 * (double)m && zeros > 0) E = (double)m * log((double)m / (double)zeros);
+        else if (E > 4294967296.0 / 30.0) E = -4294967296.0 * log(1.0 - E / 4294967296.0);
+    } else {
+        if (E <= 2.5 * (double)m) {
+            if (zeros > 0) E = (double)m * log((double)m / (double)zeros);
+        }
+        const double two64 = 18446744073709551616.0;
+        if (E > two64 / 30.0) E = -two64 * log(1.0 - E / two64);
+    }
+    return E;
+}
+
+// One group of L lanes per HLL edge, the group's lanes striding over the two
+// 2^p-byte rows with 16-byte loads.
+//   ONEPASS (p <= 10, where most edges need every register): one pass over
+//     both rows forms the zero count and the exact sum together.
+//   otherwise: pass 1 counts the zero registers V of the merged row from the
+//     AND of the two rows' zero masks (ZM; else from the registers).  Every
+//     zero register adds exactly 1 to Z = sum 2^-r, so V >= lc_min (the
+//     smallest V with alpha*m^2/V <= 2.5m, with a 1e-9 margin for the FP64
+//     comparison) proves the estimator takes its linear-counting branch: E =
+//     m * ln(m / V), the same expression the full estimator evaluates, and Z
+//     is not needed.  Otherwise pass 2 forms Z exactly and applies the full
+//     estimator.
+// CACHE: each group takes a contiguous run of the edge list.  The routing
+// pass appends edges in CSR order, so consecutive HLL edges mostly share u
+// and the group keeps u's zero mask in registers across them (up to four
+// 16-byte words per lane).  Otherwise the groups stride over the list.
+template <int L, bool ZM, bool CACHE, bool ONEPASS>
 __global__ void __launch_bounds__(256, CACHE ? 3 : 4) hll_edges_kernel(const HllParams H) {
     const int lane = threadIdx.x & 31;
     const int sub = lane & (L - 1);
@@ -1099,10 +1423,6 @@ __global__ void __launch_bounds__(256, CACHE ? 3 : 4) hll_edges_kernel(const Hll
     const int S = 65 - H.p;
     U128 hacc;
     int64_t n_approx = 0, n_clamped = 0;
-    // CACHE: each group takes a contiguous run of the edge list.  The routing
-    // pass appends edges in CSR order, so consecutive HLL edges mostly share u
-    // and the group keeps u's zero mask in registers across them (up to four
-    // 16-byte words per lane).  Otherwise the groups stride over the list.
     const int64_t per = CACHE ? (n + ngroups - 1) / ngroups : 1;
     const int64_t e_lo = CACHE ? gid * per : gid;
     const int64_t e_hi = CACHE ? min(n, e_lo + per) : n;
@@ -1117,81 +1437,91 @@ __global__ void __launch_bounds__(256, CACHE ? 3 : 4) hll_edges_kernel(const Hll
         const int64_t sv = H.slot ? __ldg(H.slot + v) : (int64_t)v;
         const uint4* a4 = reinterpret_cast<const uint4*>(H.regs + su * (int64_t)m);
         const uint4* b4 = reinterpret_cast<const uint4*>(H.regs + sv * (int64_t)m);
-        uint32_t zeros = 0;
-        if (ZM) {  // registers zero in both rows: AND of the two zero masks
-            const uint4* za = reinterpret_cast<const uint4*>(H.zm + su * (int64_t)H.zst);
-            const uint4* zb = reinterpret_cast<const uint4*>(H.zm + sv * (int64_t)H.zst);
-            if (cache_a) {
-                if (su != cached) {  // group-uniform
+        double E;
+        if (ONEPASS) {
+            uint32_t fast = 0, zeros = 0;
+            uint64_t fine = 0;
+            double extra = 0.0;
+#pragma unroll 4
+            for (int i = sub; i < nvec; i += L) {
+                const uint4 a = __ldg(a4 + i), b = __ldg(b4 + i);
+                hll_word_lut(__vmaxu4(a.x, b.x), S, fast, fine, zeros, extra);
+                hll_word_lut(__vmaxu4(a.y, b.y), S, fast, fine, zeros, extra);
+                hll_word_lut(__vmaxu4(a.z, b.z), S, fast, fine, zeros, extra);
+                hll_word_lut(__vmaxu4(a.w, b.w), S, fast, fine, zeros, extra);
+            }
+            fast = group_sum_u32<L>(fast, gmask);
+            zeros = group_sum_u32<L>(zeros, gmask);
+            fine = group_sum_u64<L>(fine, gmask);
+#pragma unroll
+            for (int o = L / 2; o > 0; o >>= 1) extra += __shfl_xor_sync(gmask, extra, o);
+            U128 z;  // fast * 2^(S-7) + fine; fast <= 2^(p+7)
+            z.lo = (uint64_t)fast << (S - 7);
+            z.hi = (uint64_t)fast >> (71 - S);
+            z.add(fine);
+            E = hll_estimate_from(z, extra, zeros, H.p, S, H.variant);
+        } else {
+            uint32_t zeros = 0;
+            if (ZM) {  // registers zero in both rows: AND of the two zero masks
+                const uint4* za = reinterpret_cast<const uint4*>(H.zm + su * (int64_t)H.zst);
+                const uint4* zb = reinterpret_cast<const uint4*>(H.zm + sv * (int64_t)H.zst);
+                if (cache_a) {
+                    if (su != cached) {  // group-uniform
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            const int i = sub + k * L;
+                            ca[k] = i < nq ? __ldg(za + i) : make_uint4(0u, 0u, 0u, 0u);
+                        }
+                        cached = su;
+                    }
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
                         const int i = sub + k * L;
-                        ca[k] = i < nq ? __ldg(za + i) : make_uint4(0u, 0u, 0u, 0u);
+                        if (i < nq) {
+                            const uint4 b = __ldg(zb + i);
+                            zeros += __popc(ca[k].x & b.x) + __popc(ca[k].y & b.y) + __popc(ca[k].z & b.z) +
+                                     __popc(ca[k].w & b.w);
+                        }
                     }
-                    cached = su;
-                }
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const int i = sub + k * L;
-                    if (i < nq) {
-                        const uint4 b = __ldg(zb + i);
-                        zeros += __popc(ca[k].x & b.x) + __popc(ca[k].y & b.y) + __popc(ca[k].z & b.z) +
-                                 __popc(ca[k].w & b.w);
+                } else {
+#pragma unroll 4
+                    for (int i = sub; i < nq; i += L) {
+                        const uint4 a = __ldg(za + i), b = __ldg(zb + i);
+                        zeros += __popc(a.x & b.x) + __popc(a.y & b.y) + __popc(a.z & b.z) + __popc(a.w & b.w);
                     }
                 }
             } else {
 #pragma unroll 4
-                for (int i = sub; i < nq; i += L) {
-                    const uint4 a = __ldg(za + i), b = __ldg(zb + i);
-                    zeros += __popc(a.x & b.x) + __popc(a.y & b.y) + __popc(a.z & b.z) + __popc(a.w & b.w);
+                for (int i = sub; i < nvec; i += L) {
+                    const uint4 a = __ldg(a4 + i), b = __ldg(b4 + i);
+                    zeros += zero_bytes(a.x | b.x) + zero_bytes(a.y | b.y) + zero_bytes(a.z | b.z) +
+                             zero_bytes(a.w | b.w);
                 }
             }
-        } else {
-#pragma unroll 4
-            for (int i = sub; i < nvec; i += L) {
-                const uint4 a = __ldg(a4 + i), b = __ldg(b4 + i);
-                zeros += zero_bytes(a.x | b.x) + zero_bytes(a.y | b.y) + zero_bytes(a.z | b.z) +
-                         zero_bytes(a.w | b.w);
-            }
-        }
-        zeros = group_sum_u32<L>(zeros, gmask);
-        double E;
-        if (zeros >= H.lc_min) {
-            E = (double)m * log((double)m / (double)zeros);
-        } else {
-            U128 sum;
-            double extra = 0.0;
+            zeros = group_sum_u32<L>(zeros, gmask);
+            if (zeros >= H.lc_min) {
+                E = (double)m * log((double)m / (double)zeros);
+            } else {
+                uint32_t fast = 0, zz = 0;
+                uint64_t fine = 0;
+                double extra = 0.0;
 #pragma unroll 2
-            for (int i = sub; i < nvec; i += L) {
-                const uint4 a = __ldg(a4 + i), b = __ldg(b4 + i);
-                hll_word128(__vmaxu4(a.x, b.x), S, sum, extra);
-                hll_word128(__vmaxu4(a.y, b.y), S, sum, extra);
-                hll_word128(__vmaxu4(a.z, b.z), S, sum, extra);
-                hll_word128(__vmaxu4(a.w, b.w), S, sum, extra);
-            }
-            sum = group_sum_u128<L>(sum, gmask);
-#pragma unroll
-            for (int o = L / 2; o > 0; o >>= 1) extra += __shfl_xor_sync(gmask, extra, o);
-            U128 z;
-            z.lo = (uint64_t)zeros << S;
-            z.hi = (uint64_t)zeros >> (64 - S);
-            sum.add(z);
-            const double Z = ldexp(u128_to_double(sum.lo, sum.hi) + extra, -S);
-            double alpha;
-            if (m == 16) alpha = 0.673;
-            else if (m == 32) alpha = 0.697;
-            else if (m == 64) alpha = 0.709;
-            else alpha = 0.7213 / (1.0 + 1.079 / (double)m);
-            E = alpha * (double)m * (double)m / Z;
-            if (H.variant == 1) {
-                if (E <= 2.5 * (double)m && zeros > 0) E = (double)m * log((double)m / (double)zeros);
-                else if (E > 4294967296.0 / 30.0) E = -4294967296.0 * log(1.0 - E / 4294967296.0);
-            } else {
-                if (E <= 2.5 * (double)m) {
-                    if (zeros > 0) E = (double)m * log((double)m / (double)zeros);
+                for (int i = sub; i < nvec; i += L) {
+                    const uint4 a = __ldg(a4 + i), b = __ldg(b4 + i);
+                    hll_word_lut(__vmaxu4(a.x, b.x), S, fast, fine, zz, extra);
+                    hll_word_lut(__vmaxu4(a.y, b.y), S, fast, fine, zz, extra);
+                    hll_word_lut(__vmaxu4(a.z, b.z), S, fast, fine, zz, extra);
+                    hll_word_lut(__vmaxu4(a.w, b.w), S, fast, fine, zz, extra);
                 }
-                const double two64 = 18446744073709551616.0;
-                if (E > two64 / 30.0) E = -two64 * log(1.0 - E / two64);
+                fast = group_sum_u32<L>(fast, gmask);
+                fine = group_sum_u64<L>(fine, gmask);
+#pragma unroll
+                for (int o = L / 2; o > 0; o >>= 1) extra += __shfl_xor_sync(gmask, extra, o);
+                U128 z;
+                z.lo = (uint64_t)fast << (S - 7);
+                z.hi = (uint64_t)fast >> (71 - S);
+                z.add(fine);
+                E = hll_estimate_from(z, extra, zeros, H.p, S, H.variant);
             }
         }
         if (sub == 0) {
@@ -1229,54 +1559,101 @@ struct Tuning {
     int warps = 8;          // warps per CTA
     int pairs = 1;          // table-side / probe-side reorientation
     int sparse = 0;         // table load <= 1/4 where it fits
-    int hub = 128;          // pairs with d+(x) > hub go to the CTA-table kernel (0: off)
+    int hub = 128;          // pairs with d+(x) > hub go to the CTA-table kernels (0: off)
     int hub_seg = 2048;     // hub pairs per CTA work unit
-    int hub_lg = 13;        // largest CTA table: 2^13 slots = 32 KB
+    int hub_lg = 13;        // largest CTA hash table: 2^13 slots = 32 KB
     int hub_unroll = 2;     // quads per lane in flight (2 or 4)
+    int bitmap_lg = 15;     // hub bitmap buffer: 2^15 bytes = 262,144 core vertices (0: hash tables only)
+    int overlap = 1;        // hybrid: HLL pass on a side stream beside the exact pairs
+    int hll_onepass_p = 10; // HLL pass: one pass over both register rows for p <= this
+    int hll_lanes = 0;      // HLL pass: lanes per edge (0: chosen by p)
 };
 constexpr int HUB_MIN = 64;       // smallest hub threshold (bounds the segment count)
 constexpr int HUB_SEG_MIN = 256;  // smallest segment
+
+// The launch shape is process-wide state set through tchll_set_count_*.
+// Every counting call copies it once, under the lock, and uses only its
+// copy, so a concurrent setter can never change a shape half-way through a
+// launch sequence (e.g. a table size versus its shared-memory allocation).
+static std::mutex g_tuning_mu;
 static Tuning g_tuning;
+static Tuning tuning_snapshot() {
+    std::lock_guard<std::mutex> lock(g_tuning_mu);
+    return g_tuning;
+}
+
+// Opts a kernel into `smem` bytes of dynamic shared memory once per device
+// (the attribute is per device and function); `done` is that kernel's
+// per-device high-water mark, guarded by its own lock.
+static std::mutex g_attr_mu;
+static int ensure_smem(const void* kern, size_t smem, size_t* done, const char* what, bool carveout = false) {
+    const int dev = current_device();
+    if (dev < 0) return cuda_status(cudaErrorInvalidDevice, "cudaGetDevice");
+    std::lock_guard<std::mutex> lock(g_attr_mu);
+    if (smem > done[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return cuda_status(e, what);
+        if (carveout) {
+            e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+            if (e != cudaSuccess) return cuda_status(e, what);
+        }
+        done[dev] = smem;
+    }
+    return TCHLL_OK;
+}
 
 // Optional phase timing: CUDA events recorded on the caller's stream around
-// the pair regrouping, the exact-count launch and the HLL launch.
+// the pair regrouping, the exact-count launch and the HLL launch.  While
+// timing is on, counting calls hold g_phase_mu for their whole enqueue, so
+// the events and flags belong to one call at a time.
 struct PhaseTimer {
-    bool on = false;
+    std::atomic<bool> on{false};
     bool made = false;
     cudaEvent_t ev[4];
-    cudaEvent_t hub_ev[2];  // around the hub kernel, inside phase 1
+    cudaEvent_t hub_ev[3];  // core pass start, hub kernels start, hub kernels end (inside phase 1)
+    cudaEvent_t hll_ev[2];  // around the HLL pass when it runs on the side stream
     bool used[3] = {false, false, false};
     bool hub_used = false;
+    bool hll_split = false;  // phase 2 (HLL) is timed by hll_ev, not ev[2..3]
 };
 static PhaseTimer g_phase;
+static std::mutex g_phase_mu;
 
-static void phase_mark(int i, cudaStream_t st) {
-    if (g_phase.on && g_phase.made) cudaEventRecord(g_phase.ev[i], st);
+// Lock held by a counting call while it records phase events.
+struct PhaseScope {
+    std::unique_lock<std::mutex> lock;
+    PhaseScope() : lock(g_phase_mu, std::defer_lock) {
+        if (g_phase.on.load()) lock.lock();
+    }
+    bool active() const { return lock.owns_lock() && g_phase.made; }
+};
+
+static void phase_mark(const PhaseScope& ps, int i, cudaStream_t st) {
+    if (ps.active()) cudaEventRecord(g_phase.ev[i], st);
 }
-static void phase_reset() {
+static void phase_used(const PhaseScope& ps, int a, int b = -1, int c = -1) {
+    if (!ps.active()) return;
+    for (int i : {a, b, c})
+        if (i >= 0) g_phase.used[i] = true;
+}
+static void phase_reset(const PhaseScope& ps) {
+    if (!ps.active()) return;
     for (int i = 0; i < 3; ++i) g_phase.used[i] = false;
     g_phase.hub_used = false;
+    g_phase.hll_split = false;
 }
 
 template <int MODE, bool VEC, bool DETAILS>
-static int launch_mode(const CountParams& P, cudaStream_t st) {
+static int launch_mode(const CountParams& P, const Tuning& T, cudaStream_t st) {
     auto kern = count_kernel<MODE, VEC, DETAILS>;
-    const int threads = g_tuning.warps * 32;
-    const size_t smem = (size_t)g_tuning.warps * ((size_t)1 << P.slots_log2) * sizeof(int32_t);
-    // largest dynamic smem opted into so far, per device (the attribute is
-    // per device; a process may drive several)
+    const int threads = T.warps * 32;
+    const size_t smem = (size_t)T.warps * ((size_t)1 << P.slots_log2) * sizeof(int32_t);
     static size_t smem_set[kMaxDevices] = {};
-    const int dev = current_device();
-    cudaError_t e;
-    if (dev < 0) return cuda_status(cudaErrorInvalidDevice, "cudaGetDevice");
-    if (smem > smem_set[dev]) {
-        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(count_kernel)");
-        smem_set[dev] = smem;
-    }
-    int bps = g_tuning.blocks_per_sm;
+    int rc = ensure_smem((const void*)kern, smem, smem_set, "cudaFuncSetAttribute(count_kernel)");
+    if (rc) return rc;
+    int bps = T.blocks_per_sm;
     if (bps <= 0) {
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, threads, smem);
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, threads, smem);
         if (e != cudaSuccess) return cuda_status(e, "occupancy(count_kernel)");
         if (bps < 1) bps = 1;
     }
@@ -1287,10 +1664,10 @@ static int launch_mode(const CountParams& P, cudaStream_t st) {
 }
 
 template <int MODE>
-static int launch_count(const CountParams& P, bool details, cudaStream_t st) {
+static int launch_count(const CountParams& P, const Tuning& T, bool details, cudaStream_t st) {
     const bool vec = ((uintptr_t)P.col_idx % 16 == 0) && (P.regs == nullptr || (uintptr_t)P.regs % 16 == 0);
-    if (details) return vec ? launch_mode<MODE, true, true>(P, st) : launch_mode<MODE, false, true>(P, st);
-    return vec ? launch_mode<MODE, true, false>(P, st) : launch_mode<MODE, false, false>(P, st);
+    if (details) return vec ? launch_mode<MODE, true, true>(P, T, st) : launch_mode<MODE, false, true>(P, T, st);
+    return vec ? launch_mode<MODE, true, false>(P, T, st) : launch_mode<MODE, false, false>(P, T, st);
 }
 
 struct CountWs {
@@ -1303,8 +1680,12 @@ struct CountWs {
     int32_t* py;              // n_edges (small pairs, then the hub list)
     HubSeg* segs;             // max_segs
     int64_t max_segs;
-    int32_t* pcol;            // padded lists for the hub kernel, pcap entries (null: not carved)
+    int32_t* pcol;            // core-filtered padded lists for the hub kernels, pcap entries (null: not carved)
     int64_t pcap;
+    int32_t* cflag;           // n_nodes + 1: core flags, then core indices (with pcol)
+    int32_t* cpos;            // n_nodes + 1: scan of the flags (with pcol)
+    int32_t* plen;            // n_nodes: filtered probe-list lengths (with pcol)
+    int32_t* ncore;           // 1: core size (with pcol)
     void* tmp;
     size_t tmp_bytes;
 };
@@ -1332,6 +1713,10 @@ static bool carve_count(void* ws, size_t bytes, int64_t n_nodes, int64_t n_edges
     W.segs = cv.take<HubSeg>((size_t)W.max_segs);
     W.pcap = pad ? pad_capacity(n_nodes, (int64_t)E) : 0;
     W.pcol = pad ? cv.take<int32_t>((size_t)W.pcap) : nullptr;
+    W.cflag = pad ? cv.take<int32_t>(N) : nullptr;
+    W.cpos = pad ? cv.take<int32_t>(N) : nullptr;
+    W.plen = pad ? cv.take<int32_t>(N) : nullptr;
+    W.ncore = pad ? cv.take<int32_t>(4) : nullptr;
     W.tmp_bytes = tb;
     W.tmp = cv.take<char>(tb);
     if (need) *need = cv.off;
@@ -1387,16 +1772,17 @@ static uint32_t lc_min_for(int p) {
 }
 
 template <int L>
-static int launch_hll_edges_L(const HllParams& H, cudaStream_t st) {
+static int launch_hll_edges_L(const HllParams& H, bool onepass, cudaStream_t st) {
     const int grid = sm_count() * 8;
-    if (H.zm && H.p >= 11) hll_edges_kernel<L, true, true><<<grid, 256, 0, st>>>(H);
-    else if (H.zm) hll_edges_kernel<L, true, false><<<grid, 256, 0, st>>>(H);
-    else hll_edges_kernel<L, false, false><<<grid, 256, 0, st>>>(H);
+    if (onepass) hll_edges_kernel<L, false, false, true><<<grid, 256, 0, st>>>(H);
+    else if (H.zm && H.p >= 11) hll_edges_kernel<L, true, true, false><<<grid, 256, 0, st>>>(H);
+    else if (H.zm) hll_edges_kernel<L, true, false, false><<<grid, 256, 0, st>>>(H);
+    else hll_edges_kernel<L, false, false, false><<<grid, 256, 0, st>>>(H);
     TCHLL_CHECK_LAUNCH("hll_edges_kernel");
     return TCHLL_OK;
 }
 
-static int launch_hll_edges(const CountParams& P, const HybridWs& HW, cudaStream_t st) {
+static int launch_hll_edges(const CountParams& P, const HybridWs& HW, const Tuning& T, cudaStream_t st) {
     HllParams H;
     H.vbase = P.graph_vbase;
     H.n_graphs = P.n_graphs;
@@ -1410,32 +1796,37 @@ static int launch_hll_edges(const CountParams& P, const HybridWs& HW, cudaStream
     H.variant = P.variant;
     H.lc_min = lc_min_for(P.p);
     H.result = P.result;
-    H.zm = HW.zm;
-    H.zst = HW.zst;
-    // Group width (lanes per edge, at most a warp).  Without zero masks: one
-    // 16-byte register load per lane per row.  With them, for p >= 11 the
-    // linear-counting shortcut settles almost every edge from the masks
+    // p <= onepass_p: one pass over both register rows (most edges need
+    // them all; no zero masks).  Otherwise the zero masks first (when the
+    // workspace holds them).
+    const bool onepass = P.p <= T.hll_onepass_p;
+    H.zm = onepass ? nullptr : HW.zm;
+    H.zst = onepass ? 0 : HW.zst;
+    // Group width (lanes per edge, at most a warp).  One pass: m / 128 lanes
+    // (p = 10: 8 lanes of 128 registers each).  With zero masks, for p >= 11
+    // the linear-counting shortcut settles almost every edge from the masks
     // alone, a pass bound by the latency of its dependent loads: four mask
-    // loads per lane per row, several edges per warp in flight.  For p = 9, 10
-    // most edges also need the register pass, which runs better on wider
-    // groups: one mask load per lane.  For p <= 8 one lane per edge.
-    // (Measured on R-MAT scale 22, theta = 256.)
+    // loads per lane per row, several edges per warp in flight.  Otherwise
+    // one 16-byte register load per lane per row.  (Measured on R-MAT scale
+    // 22, theta = 256.)  T.hll_lanes > 0 overrides the width.
     int width = (1 << P.p) >> 4;
-    if (HW.zm) width = P.p >= 11 ? HW.zst >> 4 : (P.p >= 9 ? HW.zst >> 2 : 1);
-    if (HW.zm) {
+    if (onepass) width = (1 << P.p) >> 7;
+    else if (H.zm) width = P.p >= 11 ? H.zst >> 4 : (P.p >= 9 ? H.zst >> 2 : 1);
+    if (T.hll_lanes > 0) width = T.hll_lanes;
+    if (H.zm) {
         const int64_t rows = P.slot ? P.n_rows : P.n_nodes;
         const int64_t wgrid = (rows + 7) / 8;
         const int grid = (int)(wgrid < 1 ? 1 : (wgrid > (int64_t)sm_count() * 16 ? (int64_t)sm_count() * 16 : wgrid));
-        zmask_kernel<<<grid, 256, 0, st>>>(P.regs, rows, P.slot ? nullptr : P.has, P.p, HW.zst, HW.zm);
+        zmask_kernel<<<grid, 256, 0, st>>>(P.regs, rows, P.slot ? nullptr : P.has, P.p, H.zst, HW.zm);
         TCHLL_CHECK_LAUNCH("zmask_kernel");
     }
-    switch (width >= 32 ? 32 : width) {
-        case 1: return launch_hll_edges_L<1>(H, st);
-        case 2: return launch_hll_edges_L<2>(H, st);
-        case 4: return launch_hll_edges_L<4>(H, st);
-        case 8: return launch_hll_edges_L<8>(H, st);
-        case 16: return launch_hll_edges_L<16>(H, st);
-        default: return launch_hll_edges_L<32>(H, st);
+    switch (width >= 32 ? 32 : (width < 1 ? 1 : width)) {
+        case 1: return launch_hll_edges_L<1>(H, onepass, st);
+        case 2: return launch_hll_edges_L<2>(H, onepass, st);
+        case 4: return launch_hll_edges_L<4>(H, onepass, st);
+        case 8: return launch_hll_edges_L<8>(H, onepass, st);
+        case 16: return launch_hll_edges_L<16>(H, onepass, st);
+        default: return launch_hll_edges_L<32>(H, onepass, st);
     }
 }
 
@@ -1451,7 +1842,7 @@ static int grid_edges(int64_t n) {
 // With hub > 0 the histogram is split into small and hub pairs, both are
 // scanned, and the hub segments are listed (before the scatter moves offh).
 template <bool HYB>
-static int pairs_hist_scan(const CountParams& P, const CountWs& W, int hub, cudaStream_t st,
+static int pairs_hist_scan(const CountParams& P, const CountWs& W, int hub, int hub_seg, cudaStream_t st,
                            const int32_t* vbase = nullptr, int64_t n_graphs = 0) {
     const int64_t N = P.n_nodes + 1;
     TCHLL_CUDA(cudaMemsetAsync(W.cnt, 0, sizeof(int32_t) * N, st));
@@ -1469,7 +1860,7 @@ static int pairs_hist_scan(const CountParams& P, const CountWs& W, int hub, cuda
         TCHLL_CUDA(cub::DeviceScan::ExclusiveSum(W.tmp, tb, W.cnth, W.offh, (int)N, st));
         count_launch();
         hub_segments_kernel<<<grid_edges(P.n_nodes), 256, 0, st>>>(W.cnth, W.offh, W.off + P.n_nodes, P.n_nodes,
-                                                                   g_tuning.hub_seg, W.segs, W.ctr + 2,
+                                                                   hub_seg, W.segs, W.ctr + 2,
                                                                    W.max_segs, vbase, n_graphs);
         TCHLL_CHECK_LAUNCH("hub_segments_kernel");
     }
@@ -1490,11 +1881,23 @@ static int pairs_scatter(const CountParams& P, const CountWs& W, int hub, CountP
     return TCHLL_OK;
 }
 
-// The hub pairs: one CTA per segment at a time, persistent grid.
-static int launch_hub(const CountParams& P, const CountWs& W, cudaStream_t st, bool batched = false) {
-    HubParams H;
+static int grid_rows(int64_t n, int per_cta) {  // one unit of work per 256 / per_cta threads
+    int64_t g = (n + per_cta - 1) / per_cta;
+    const int64_t cap = (int64_t)sm_count() * 16;
+    return (int)(g < 1 ? 1 : (g > cap ? cap : g));
+}
+
+// The hub pairs: one CTA per segment at a time, persistent grid.  With the
+// padded lists in the workspace: the core pass (flags, scan, indices,
+// filtered lists), then the bitmap kernel, then the hash kernel, which
+// returns at once when the bitmap kernel could hold the core.  Without them
+// (a small workspace): the hash kernel over the raw lists.
+static int launch_hub(const CountParams& P, const CountWs& W, const Tuning& T, const PhaseScope& ps, cudaStream_t st,
+                      bool batched = false) {
+    HubParams H{};
     H.batched = batched;
     H.row_ptr = P.row_ptr;
+    H.n_nodes = P.n_nodes;
     H.col_idx = P.col_idx;
     H.nnz = P.nnz;
     H.hy = W.py;
@@ -1502,69 +1905,150 @@ static int launch_hub(const CountParams& P, const CountWs& W, cudaStream_t st, b
     H.n_segs = W.ctr + 2;
     H.max_segs = W.max_segs;
     H.seg_ctr = W.ctr + 3;
-    H.hub_lg = g_tuning.hub_lg;
+    H.hub_lg = T.hub_lg;
     H.result = P.result;
-    // padded probe lists when the workspace holds them and quad indices fit int
+    // core-filtered padded lists when the workspace holds them and quad
+    // indices fit int
     const int64_t need_pad = pad_capacity(P.n_nodes, P.nnz);
     const bool pad = W.pcol != nullptr && need_pad <= W.pcap && need_pad <= (int64_t)INT32_MAX;
-    H.pcol = pad ? W.pcol : nullptr;
+    if (ps.active()) cudaEventRecord(g_phase.hub_ev[0], st);
     if (pad) {
-        int64_t g = (P.n_nodes + 31) / 32;
-        const int64_t cap = (int64_t)sm_count() * 16;
-        g = g < 1 ? 1 : (g > cap ? cap : g);
-        pad_rows_kernel<<<(int)g, 256, 0, st>>>(P.row_ptr, P.n_nodes, P.col_idx, W.pcol);
-        TCHLL_CHECK_LAUNCH("pad_rows_kernel");
+        const int64_t N = P.n_nodes + 1;
+        TCHLL_CUDA(cudaMemsetAsync(W.cflag, 0, sizeof(int32_t) * N, st));
+        core_mark_kernel<<<grid_rows(P.n_nodes, 256), 256, 0, st>>>(P.row_ptr, P.n_nodes, P.nnz, P.col_idx, W.cnth,
+                                                                     W.cflag, P.result);
+        TCHLL_CHECK_LAUNCH("core_mark_kernel");
+        size_t tb = W.tmp_bytes;
+        TCHLL_CUDA(cub::DeviceScan::ExclusiveSum(W.tmp, tb, W.cflag, W.cpos, (int)N, st));
+        count_launch();
+        core_index_kernel<<<grid_rows(N, 256), 256, 0, st>>>(W.cflag, W.cpos, P.n_nodes, W.ncore);
+        TCHLL_CHECK_LAUNCH("core_index_kernel");
+        core_pad_kernel<<<grid_rows(P.n_nodes, 8), 256, 0, st>>>(P.row_ptr, P.n_nodes, P.nnz, P.col_idx, W.cflag,
+                                                                 W.ncore, W.pcol, W.plen, P.result);
+        TCHLL_CHECK_LAUNCH("core_pad_kernel");
+        H.pcol = W.pcol;
+        H.cidx = W.cflag;
+        H.plen = W.plen;
+        H.n_core = W.ncore;
     }
-    const int vi = (g_tuning.hub_unroll == 4 ? 2 : 0) + (pad ? 1 : 0);
+    if (ps.active()) cudaEventRecord(g_phase.hub_ev[1], st);
+    if (pad && T.bitmap_lg > 0) {
+        const size_t smem = (size_t)1 << T.bitmap_lg;
+        H.cap_bits = (int)(8 * smem);
+        auto kern = T.hub_unroll == 4 ? hub_bitmap_kernel<4> : hub_bitmap_kernel<2>;
+        static size_t smem_set[2][kMaxDevices] = {};
+        int rc = ensure_smem((const void*)kern, smem, smem_set[T.hub_unroll == 4 ? 1 : 0],
+                             "cudaFuncSetAttribute(hub_bitmap_kernel)", true);
+        if (rc) return rc;
+        int bps = 0;
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, 256, smem);
+        if (e != cudaSuccess) return cuda_status(e, "occupancy(hub_bitmap_kernel)");
+        if (bps < 1) bps = 1;
+        kern<<<sm_count() * bps, 256, smem, st>>>(H);
+        TCHLL_CHECK_LAUNCH("hub_bitmap_kernel");
+    }
+    const int vi = (T.hub_unroll == 4 ? 2 : 0) + (pad ? 1 : 0);
     auto kern = vi == 3 ? hub_count_kernel<4, true>
                         : vi == 2 ? hub_count_kernel<4, false> : vi == 1 ? hub_count_kernel<2, true> : hub_count_kernel<2, false>;
-    const size_t smem = sizeof(int32_t) << g_tuning.hub_lg;
-    static size_t smem_set[kMaxDevices][4] = {};  // per device and kernel variant
-    const int dev = current_device();
-    if (dev < 0) return cuda_status(cudaErrorInvalidDevice, "cudaGetDevice");
-    size_t& done = smem_set[dev][vi];
-    cudaError_t e;
-    if (smem > done) {
-        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(hub_count_kernel)");
-        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(hub_count_kernel carveout)");
-        done = smem;
-    }
+    const size_t smem = sizeof(int32_t) << T.hub_lg;
+    static size_t hsmem_set[4][kMaxDevices] = {};
+    int rc = ensure_smem((const void*)kern, smem, hsmem_set[vi], "cudaFuncSetAttribute(hub_count_kernel)", true);
+    if (rc) return rc;
     int bps = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, 256, smem);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, 256, smem);
     if (e != cudaSuccess) return cuda_status(e, "occupancy(hub_count_kernel)");
     if (bps < 1) bps = 1;
-    if (g_phase.on && g_phase.made) cudaEventRecord(g_phase.hub_ev[0], st);
     kern<<<sm_count() * bps, 256, smem, st>>>(H);
     TCHLL_CHECK_LAUNCH("hub_count_kernel");
-    if (g_phase.on && g_phase.made) {
-        cudaEventRecord(g_phase.hub_ev[1], st);
+    if (ps.active()) {
+        cudaEventRecord(g_phase.hub_ev[2], st);
         g_phase.hub_used = true;
     }
     return TCHLL_OK;
 }
 
 // Hub path in use: pairs on, and 16-byte aligned col_idx (quad loads).
-static int hub_threshold(const CountParams& P) {
-    return (g_tuning.hub > 0 && (uintptr_t)P.col_idx % 16 == 0) ? g_tuning.hub : 0;
+static int hub_threshold(const CountParams& P, const Tuning& T) {
+    return (T.hub > 0 && (uintptr_t)P.col_idx % 16 == 0) ? T.hub : 0;
 }
 
 // Build the grouped (x, y) pair list of the exact edges into Q.
 template <bool HYB>
-static int build_pairs(const CountParams& P, const CountWs& W, int hub, CountParams& Q, cudaStream_t st) {
-    int rc = pairs_hist_scan<HYB>(P, W, hub, st);
+static int build_pairs(const CountParams& P, const CountWs& W, int hub, int hub_seg, CountParams& Q,
+                       cudaStream_t st) {
+    int rc = pairs_hist_scan<HYB>(P, W, hub, hub_seg, st);
     if (rc) return rc;
     return pairs_scatter<HYB>(P, W, hub, Q, st);
 }
 
+// A second stream per device for work that overlaps the caller's stream: the
+// HLL pass of a hybrid count runs there beside the exact pairs.  Fork = an
+// event recorded on the caller's stream that the side stream waits for;
+// join = an event recorded on the side stream that the caller's stream
+// waits for before the call returns.  Both are recorded under the device's
+// lock, held from fork to join, so concurrent calls never wait on each
+// other's events; under stream capture this is the usual fork/join of a
+// captured graph.  Stream and events are created on first use (outside any
+// capture: the first call of a process is never captured by this package).
+struct SideStream {
+    cudaStream_t s = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    std::mutex mu;
+};
+static SideStream g_side[kMaxDevices];
+static std::mutex g_side_make_mu;
+
+class SideFork {
+  public:
+    // Starts the fork (returns an error status, or TCHLL_OK with stream()
+    // ready for work that may run once the caller's stream got here).
+    int begin(cudaStream_t caller) {
+        const int dev = current_device();
+        if (dev < 0) return cuda_status(cudaErrorInvalidDevice, "cudaGetDevice");
+        SideStream& S = g_side[dev];
+        {
+            std::lock_guard<std::mutex> mk(g_side_make_mu);
+            if (S.s == nullptr) {
+                TCHLL_CUDA(cudaStreamCreateWithFlags(&S.s, cudaStreamNonBlocking));
+                TCHLL_CUDA(cudaEventCreateWithFlags(&S.fork, cudaEventDisableTiming));
+                TCHLL_CUDA(cudaEventCreateWithFlags(&S.join, cudaEventDisableTiming));
+            }
+        }
+        lock_ = std::unique_lock<std::mutex>(S.mu);
+        side_ = &S;
+        caller_ = caller;
+        TCHLL_CUDA(cudaEventRecord(S.fork, caller));
+        TCHLL_CUDA(cudaStreamWaitEvent(S.s, S.fork, 0));
+        return TCHLL_OK;
+    }
+    cudaStream_t stream() const { return side_->s; }
+    // Joins: the caller's stream waits for everything enqueued on the side
+    // stream so far.  Safe to call more than once.
+    int end() {
+        if (side_ == nullptr) return TCHLL_OK;
+        SideStream* S = side_;
+        side_ = nullptr;
+        cudaError_t e = cudaEventRecord(S->join, S->s);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(caller_, S->join, 0);
+        lock_.unlock();
+        return e == cudaSuccess ? TCHLL_OK : cuda_status(e, "side stream join");
+    }
+    ~SideFork() { end(); }
+
+  private:
+    SideStream* side_ = nullptr;
+    cudaStream_t caller_ = nullptr;
+    std::unique_lock<std::mutex> lock_;
+};
+
 static int run_count(CountParams P, int mode, bool details, void* ws, size_t ws_bytes, cudaStream_t st) {
+    const Tuning T = tuning_snapshot();
     CountWs W;
     HybridWs HW{};
     size_t need = 0;
     bool ok;
     // Optional parts, used when the workspace has room (same results): the
-    // padded probe lists of the hub kernel and, for hybrid calls, the zero
+    // core-filtered lists of the hub kernels and, for hybrid calls, the zero
     // masks that let the HLL pass test linear counting without the registers.
     if (mode == MODE_EXACT) {
         ok = carve_count(ws, ws_bytes, P.n_nodes, P.n_edges, W, &need, true);
@@ -1583,87 +2067,102 @@ static int run_count(CountParams P, int mode, bool details, void* ws, size_t ws_
     TCHLL_CUDA(cudaMemsetAsync(P.result, 0, sizeof(tchll_count_result), st));
     if (details && P.pe_support) TCHLL_CUDA(cudaMemsetAsync(P.pe_support, 0, sizeof(int64_t) * P.n_edges, st));
     if (details && P.pe_method) TCHLL_CUDA(cudaMemsetAsync(P.pe_method, 0, P.n_edges, st));
-    P.chunk = g_tuning.chunk;
-    P.slots_log2 = g_tuning.slots_log2;
-    P.tiny = g_tuning.tiny;
-    P.sparse = g_tuning.sparse;
+    P.chunk = T.chunk;
+    P.slots_log2 = T.slots_log2;
+    P.tiny = T.tiny;
+    P.sparse = T.sparse;
     P.n_edges_dev = nullptr;
     P.hll_u = nullptr;
     P.hll_v = nullptr;
     P.hll_n = nullptr;
     if (P.n_edges == 0) return TCHLL_OK;
-    const bool pairs = g_tuning.pairs && !details;
+    const bool pairs = T.pairs && !details;
     int rc;
     CountParams Q;
-    phase_reset();
+    PhaseScope ps;
+    phase_reset(ps);
     switch (mode) {
         case MODE_EXACT:
             P.work = W.ctr;
             if (pairs) {
-                const int hub = hub_threshold(P);
-                phase_mark(0, st);
-                rc = build_pairs<false>(P, W, hub, Q, st);
+                const int hub = hub_threshold(P, T);
+                phase_mark(ps, 0, st);
+                rc = build_pairs<false>(P, W, hub, T.hub_seg, Q, st);
                 if (rc) return rc;
-                phase_mark(1, st);
-                rc = launch_count<MODE_EXACT>(Q, false, st);
-                if (rc == TCHLL_OK && hub > 0) rc = launch_hub(P, W, st);
-                phase_mark(2, st);
-                g_phase.used[0] = g_phase.used[1] = true;
+                phase_mark(ps, 1, st);
+                rc = launch_count<MODE_EXACT>(Q, T, false, st);
+                if (rc == TCHLL_OK && hub > 0) rc = launch_hub(P, W, T, ps, st);
+                phase_mark(ps, 2, st);
+                phase_used(ps, 0, 1);
                 return rc;
             }
-            phase_mark(1, st);
-            rc = launch_count<MODE_EXACT>(P, details, st);
-            phase_mark(2, st);
-            g_phase.used[1] = true;
+            phase_mark(ps, 1, st);
+            rc = launch_count<MODE_EXACT>(P, T, details, st);
+            phase_mark(ps, 2, st);
+            phase_used(ps, 1);
             return rc;
         case MODE_HYBRID:  // one fused launch over the edges as given
             P.work = W.ctr;
-            phase_mark(1, st);
-            rc = launch_count<MODE_HYBRID>(P, details, st);
-            phase_mark(2, st);
-            g_phase.used[1] = true;
+            phase_mark(ps, 1, st);
+            rc = launch_count<MODE_HYBRID>(P, T, details, st);
+            phase_mark(ps, 2, st);
+            phase_used(ps, 1);
             return rc;
         case 2:  // split: exact-routed edges, then HLL-routed edges
             if (pairs && ((uintptr_t)P.regs % 16 == 0)) {
                 // One routing pass builds both work lists: the exact pairs
-                // (counted by the pair launch, which also counts n_exact) and
-                // the HLL edge list (estimated by hll_edges_kernel, which
+                // (counted by the pair launches, which also count n_exact)
+                // and the HLL edge list (estimated by hll_edges_kernel, which
                 // counts n_approx / n_clamped); the routing pass counts
-                // n_fallback.
+                // n_fallback.  The HLL pass needs only the routing pass, so
+                // it forks onto the side stream there and overlaps the
+                // scatter and the pair launches (all add integers into the
+                // same result block).
                 P.work = W.ctr;
                 P.hll_u = HW.hll_u;
                 P.hll_v = HW.hll_v;
                 P.hll_n = HW.hll_n;
                 TCHLL_CUDA(cudaMemsetAsync(HW.hll_n, 0, sizeof(unsigned long long), st));
-                const int hub = hub_threshold(P);
-                phase_mark(0, st);
-                rc = pairs_hist_scan<true>(P, W, hub, st);
+                const int hub = hub_threshold(P, T);
+                phase_mark(ps, 0, st);
+                rc = pairs_hist_scan<true>(P, W, hub, T.hub_seg, st);
+                if (rc) return rc;
+                SideFork fork;
+                cudaStream_t hst = st;
+                if (T.overlap) {
+                    rc = fork.begin(st);
+                    if (rc) return rc;
+                    hst = fork.stream();
+                }
+                if (ps.active()) cudaEventRecord(g_phase.hll_ev[0], hst);
+                rc = launch_hll_edges(P, HW, T, hst);
+                if (ps.active()) cudaEventRecord(g_phase.hll_ev[1], hst);
                 if (rc) return rc;
                 rc = pairs_scatter<true>(P, W, hub, Q, st);
                 if (rc) return rc;
-                phase_mark(1, st);
+                phase_mark(ps, 1, st);
                 Q.hll_u = nullptr;
-                rc = launch_count<MODE_EXACT>(Q, false, st);
+                rc = launch_count<MODE_EXACT>(Q, T, false, st);
                 if (rc) return rc;
                 if (hub > 0) {
-                    rc = launch_hub(P, W, st);
+                    rc = launch_hub(P, W, T, ps, st);
                     if (rc) return rc;
                 }
-                phase_mark(2, st);
-                rc = launch_hll_edges(P, HW, st);
-                phase_mark(3, st);
-                g_phase.used[0] = g_phase.used[1] = g_phase.used[2] = true;
+                phase_mark(ps, 2, st);
+                rc = fork.end();
+                phase_used(ps, 0, 1, 2);
+                if (ps.active()) g_phase.hll_split = true;
                 return rc;
             }
             P.work = W.ctr;
-            phase_mark(1, st);
-            rc = launch_count<MODE_HYB_EXACT>(P, details, st);
+            phase_mark(ps, 1, st);
+            rc = launch_count<MODE_HYB_EXACT>(P, T, details, st);
             if (rc) return rc;
-            phase_mark(2, st);
+            phase_mark(ps, 2, st);
             P.work = W.ctr + 1;
-            rc = launch_count<MODE_HYB_HLL>(P, details, st);
-            phase_mark(3, st);
-            g_phase.used[1] = g_phase.used[2] = true;
+            rc = launch_count<MODE_HYB_HLL>(P, T, details, st);
+            phase_mark(ps, 3, st);
+            phase_used(ps, 1, 2);
             return rc;
         default:
             set_error("unknown count mode %d", mode);
@@ -1787,6 +2286,7 @@ TCHLL_EXPORT int tchll_hybrid_count_compact(const int32_t* row_ptr, int64_t n_no
 }
 
 TCHLL_EXPORT int tchll_set_count_tuning(int32_t chunk, int32_t slots_log2, int32_t tiny, int32_t blocks_per_sm) {
+    std::lock_guard<std::mutex> lock(g_tuning_mu);
     TCHLL_ARG(chunk >= 32 && chunk % 32 == 0 && chunk <= (1 << 20), "chunk must be a multiple of 32 in [32, 2^20]");
     TCHLL_ARG(tiny >= 0 && tiny <= 4096, "tiny must be in [0, 4096]");
     TCHLL_ARG(blocks_per_sm >= 0 && blocks_per_sm <= 32, "blocks_per_sm must be in [0, 32]");
@@ -1800,6 +2300,7 @@ TCHLL_EXPORT int tchll_set_count_tuning(int32_t chunk, int32_t slots_log2, int32
 }
 
 TCHLL_EXPORT int tchll_set_count_shape(int32_t warps_per_cta, int32_t pairs) {
+    std::lock_guard<std::mutex> lock(g_tuning_mu);
     TCHLL_ARG(warps_per_cta >= 1 && warps_per_cta <= 8, "warps_per_cta must be in [1, 8]");
     TCHLL_ARG((size_t)warps_per_cta * ((size_t)4 << g_tuning.slots_log2) <= 227 * 1024,
               "warps x 2^slots_log2 x 4 bytes must fit 227 KB of shared memory");
@@ -1809,11 +2310,13 @@ TCHLL_EXPORT int tchll_set_count_shape(int32_t warps_per_cta, int32_t pairs) {
 }
 
 TCHLL_EXPORT int tchll_set_count_table(int32_t sparse) {
+    std::lock_guard<std::mutex> lock(g_tuning_mu);
     g_tuning.sparse = sparse ? 1 : 0;
     return TCHLL_OK;
 }
 
 TCHLL_EXPORT int tchll_set_count_hub(int32_t threshold, int32_t seg_pairs, int32_t table_log2, int32_t unroll) {
+    std::lock_guard<std::mutex> lock(g_tuning_mu);
     TCHLL_ARG(threshold == 0 || threshold >= HUB_MIN, "hub threshold must be 0 (off) or >= %d", HUB_MIN);
     TCHLL_ARG(seg_pairs >= HUB_SEG_MIN && seg_pairs <= (1 << 20), "seg_pairs must be in [%d, 2^20]", HUB_SEG_MIN);
     TCHLL_ARG(table_log2 >= 10 && table_log2 <= 15, "table_log2 must be in [10, 15]");
@@ -1827,55 +2330,104 @@ TCHLL_EXPORT int tchll_set_count_hub(int32_t threshold, int32_t seg_pairs, int32
 
 TCHLL_EXPORT int tchll_get_count_hub(int32_t* out4) {
     TCHLL_ARG(out4 != nullptr, "null output");
-    out4[0] = g_tuning.hub;
-    out4[1] = g_tuning.hub_seg;
-    out4[2] = g_tuning.hub_lg;
-    out4[3] = g_tuning.hub_unroll;
+    const Tuning T = tuning_snapshot();
+    out4[0] = T.hub;
+    out4[1] = T.hub_seg;
+    out4[2] = T.hub_lg;
+    out4[3] = T.hub_unroll;
+    return TCHLL_OK;
+}
+
+TCHLL_EXPORT int tchll_set_count_core(int32_t bitmap_log2, int32_t overlap) {
+    std::lock_guard<std::mutex> lock(g_tuning_mu);
+    TCHLL_ARG(bitmap_log2 == 0 || (bitmap_log2 >= 10 && bitmap_log2 <= 17),
+              "bitmap_log2 must be 0 (hash tables only) or in [10, 17] (1 KB .. 128 KB of shared memory)");
+    g_tuning.bitmap_lg = bitmap_log2;
+    g_tuning.overlap = overlap ? 1 : 0;
+    return TCHLL_OK;
+}
+
+TCHLL_EXPORT int tchll_get_count_core(int32_t* out2) {
+    TCHLL_ARG(out2 != nullptr, "null output");
+    const Tuning T = tuning_snapshot();
+    out2[0] = T.bitmap_lg;
+    out2[1] = T.overlap;
+    return TCHLL_OK;
+}
+
+TCHLL_EXPORT int tchll_set_hll_pass(int32_t onepass_max_p, int32_t lanes) {
+    std::lock_guard<std::mutex> lock(g_tuning_mu);
+    TCHLL_ARG(onepass_max_p >= 0 && onepass_max_p <= 16, "onepass_max_p must be in [0, 16]");
+    TCHLL_ARG(lanes == 0 || (lanes >= 1 && lanes <= 32 && (lanes & (lanes - 1)) == 0),
+              "lanes must be 0 (automatic) or a power of two in [1, 32]");
+    g_tuning.hll_onepass_p = onepass_max_p;
+    g_tuning.hll_lanes = lanes;
+    return TCHLL_OK;
+}
+
+TCHLL_EXPORT int tchll_get_hll_pass(int32_t* out2) {
+    TCHLL_ARG(out2 != nullptr, "null output");
+    const Tuning T = tuning_snapshot();
+    out2[0] = T.hll_onepass_p;
+    out2[1] = T.hll_lanes;
     return TCHLL_OK;
 }
 
 TCHLL_EXPORT int tchll_get_count_tuning(int32_t* out8) {
     TCHLL_ARG(out8 != nullptr, "out is null");
-    out8[0] = g_tuning.chunk;
-    out8[1] = g_tuning.slots_log2;
-    out8[2] = g_tuning.tiny;
-    out8[3] = g_tuning.blocks_per_sm;
-    out8[4] = g_tuning.warps;
-    out8[5] = g_tuning.pairs;
-    out8[6] = g_tuning.sparse;
+    const Tuning T = tuning_snapshot();
+    out8[0] = T.chunk;
+    out8[1] = T.slots_log2;
+    out8[2] = T.tiny;
+    out8[3] = T.blocks_per_sm;
+    out8[4] = T.warps;
+    out8[5] = T.pairs;
+    out8[6] = T.sparse;
     out8[7] = 0;  // reserved
     return TCHLL_OK;
 }
 
 TCHLL_EXPORT int tchll_set_phase_timing(int32_t enable) {
+    std::lock_guard<std::mutex> lock(g_phase_mu);
     if (enable && !g_phase.made) {
         for (int i = 0; i < 4; ++i) TCHLL_CUDA(cudaEventCreate(&g_phase.ev[i]));
-        for (int i = 0; i < 2; ++i) TCHLL_CUDA(cudaEventCreate(&g_phase.hub_ev[i]));
+        for (int i = 0; i < 3; ++i) TCHLL_CUDA(cudaEventCreate(&g_phase.hub_ev[i]));
+        for (int i = 0; i < 2; ++i) TCHLL_CUDA(cudaEventCreate(&g_phase.hll_ev[i]));
         g_phase.made = true;
     }
     g_phase.on = enable != 0;
-    phase_reset();
+    for (int i = 0; i < 3; ++i) g_phase.used[i] = false;
+    g_phase.hub_used = false;
+    g_phase.hll_split = false;
     return TCHLL_OK;
 }
 
 TCHLL_EXPORT int tchll_phase_times(float* ms3) {
     TCHLL_ARG(ms3 != nullptr, "out is null");
+    std::lock_guard<std::mutex> lock(g_phase_mu);
     for (int i = 0; i < 3; ++i) ms3[i] = -1.0f;
     if (!g_phase.on || !g_phase.made) return TCHLL_OK;
     for (int i = 0; i < 3; ++i) {
         if (!g_phase.used[i]) continue;
+        if (i == 2 && g_phase.hll_split) {  // the HLL pass ran beside phase 1
+            TCHLL_CUDA(cudaEventSynchronize(g_phase.hll_ev[1]));
+            TCHLL_CUDA(cudaEventElapsedTime(&ms3[i], g_phase.hll_ev[0], g_phase.hll_ev[1]));
+            continue;
+        }
         TCHLL_CUDA(cudaEventSynchronize(g_phase.ev[i + 1]));
         TCHLL_CUDA(cudaEventElapsedTime(&ms3[i], g_phase.ev[i], g_phase.ev[i + 1]));
     }
     return TCHLL_OK;
 }
 
-TCHLL_EXPORT int tchll_phase_hub_ms(float* ms) {
-    TCHLL_ARG(ms != nullptr, "out is null");
-    *ms = -1.0f;
+TCHLL_EXPORT int tchll_phase_hub_ms(float* ms2) {
+    TCHLL_ARG(ms2 != nullptr, "out is null");
+    std::lock_guard<std::mutex> lock(g_phase_mu);
+    ms2[0] = ms2[1] = -1.0f;
     if (!g_phase.on || !g_phase.made || !g_phase.hub_used) return TCHLL_OK;
-    TCHLL_CUDA(cudaEventSynchronize(g_phase.hub_ev[1]));
-    TCHLL_CUDA(cudaEventElapsedTime(ms, g_phase.hub_ev[0], g_phase.hub_ev[1]));
+    TCHLL_CUDA(cudaEventSynchronize(g_phase.hub_ev[2]));
+    TCHLL_CUDA(cudaEventElapsedTime(&ms2[0], g_phase.hub_ev[1], g_phase.hub_ev[2]));
+    TCHLL_CUDA(cudaEventElapsedTime(&ms2[1], g_phase.hub_ev[0], g_phase.hub_ev[1]));
     return TCHLL_OK;
 }
 
@@ -1889,27 +2441,69 @@ TCHLL_EXPORT int tchll_phase_hub_ms(float* ms) {
 // that loads the library reserves the array until the process exits.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[TCHLL_NOALLOC_SCRATCH_BYTES];
 
-static std::mutex g_noalloc_mu;
-static void* g_noalloc_ptr[256];  // device address of the array, per device
-
 // Host code must not pass g_noalloc_scratch itself to a kernel (on the host
-// the name stands for a host-side shadow, not the device array): look the
-// device address up once per device, with that device current.
+// the name stands for a host-side shadow, not the device array): the device
+// address comes from cudaGetSymbolAddress, with the device current.  The
+// address belongs to the module as loaded in one CUDA context, so it is
+// cached per context, keyed by the context's process-unique id (cuCtxGetId,
+// reached through the runtime's driver entry-point query, so the library
+// needs no driver link): a non-primary context made current by a caller, or
+// a primary context re-created after cudaDeviceReset, gets its own lookup.
+// Where the id cannot be read, every call looks the address up again.
+static std::mutex g_noalloc_mu;
+struct NoallocEntry {
+    unsigned long long ctx_id;
+    void* ptr;
+};
+static NoallocEntry g_noalloc_cache[64];
+static int g_noalloc_used = 0;
+
+typedef int (*CtxGetCurrentFn)(void** ctx);
+typedef int (*CtxGetIdFn)(void* ctx, unsigned long long* id);
+
+// Id of the calling thread's current context; false when unavailable.
+static bool current_ctx_id(unsigned long long* id) {
+    static CtxGetCurrentFn get_cur = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_cur = (CtxGetCurrentFn)f;
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = (CtxGetIdFn)f;
+    });
+    if (get_cur == nullptr || get_id == nullptr) return false;
+    void* ctx = nullptr;
+    if (get_cur(&ctx) != 0 || ctx == nullptr) return false;
+    return get_id(ctx, id) == 0;
+}
+
 static int noalloc_scratch_ptr(void** out) {
     int dev = -1;
-    TCHLL_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 256) {
-        set_error("device ordinal %d out of range", dev);
-        return TCHLL_EINVAL;
-    }
+    TCHLL_CUDA(cudaGetDevice(&dev));  // also makes the runtime's context current
+    unsigned long long id = 0;
+    const bool have_id = current_ctx_id(&id);
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (g_noalloc_ptr[dev] == nullptr) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return cuda_status(e, "cudaGetSymbolAddress(noalloc scratch)");
-        g_noalloc_ptr[dev] = p;
+    if (have_id) {
+        for (int i = 0; i < g_noalloc_used; ++i)
+            if (g_noalloc_cache[i].ctx_id == id) {
+                *out = g_noalloc_cache[i].ptr;
+                return TCHLL_OK;
+            }
     }
-    *out = g_noalloc_ptr[dev];
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_status(e, "cudaGetSymbolAddress(noalloc scratch)");
+    if (have_id) {  // a full table gives up the entry the id hashes to
+        const int slot = g_noalloc_used < 64 ? g_noalloc_used++ : (int)(id % 64);
+        g_noalloc_cache[slot] = NoallocEntry{id, p};
+    }
+    *out = p;
     return TCHLL_OK;
 }
 
@@ -2053,8 +2647,7 @@ static bool carve_batch(void* ws, size_t bytes, int64_t n_nodes, int64_t n_edges
 
 // Chunk list over per-graph ranges [base[vbase[g]], base[vbase[g+1]]).
 static int build_chunks(const int32_t* base, const int32_t* vbase, int64_t n_graphs, int64_t n_nodes,
-                        const BatchWs& B, cudaStream_t st) {
-    const int chunk = g_tuning.chunk;
+                        const BatchWs& B, int chunk, cudaStream_t st) {
     int64_t g = (n_graphs + 256) / 256;
     if (g > (int64_t)sm_count() * 8) g = (int64_t)sm_count() * 8;
     chunk_count_kernel<<<(int)g, 256, 0, st>>>(base, vbase, n_graphs, n_nodes, chunk, B.cnt);
@@ -2073,6 +2666,7 @@ static int build_chunks(const int32_t* base, const int32_t* vbase, int64_t n_gra
 
 static int run_batch(CountParams P, bool hybrid, const int32_t* vbase, int64_t n_graphs, void* ws, size_t wsb,
                      cudaStream_t st) {
+    const Tuning T = tuning_snapshot();
     BatchWs B;
     size_t need = 0;
     if (!carve_batch(ws, wsb, P.n_nodes, P.n_edges, n_graphs, B, &need) || ws == nullptr) {
@@ -2088,10 +2682,10 @@ static int run_batch(CountParams P, bool hybrid, const int32_t* vbase, int64_t n
         check_vbase_kernel<<<(int)g, 256, 0, st>>>(vbase, n_graphs, P.n_nodes, P.result);
         TCHLL_CHECK_LAUNCH("check_vbase_kernel");
     }
-    P.chunk = g_tuning.chunk;
-    P.slots_log2 = g_tuning.slots_log2;
-    P.tiny = g_tuning.tiny;
-    P.sparse = g_tuning.sparse;
+    P.chunk = T.chunk;
+    P.slots_log2 = T.slots_log2;
+    P.tiny = T.tiny;
+    P.sparse = T.sparse;
     P.n_edges_dev = nullptr;
     P.graph_vbase = vbase;
     P.n_graphs = n_graphs;
@@ -2102,7 +2696,8 @@ static int run_batch(CountParams P, bool hybrid, const int32_t* vbase, int64_t n
     if (P.n_edges == 0) return TCHLL_OK;
     int rc;
     CountParams Q;
-    phase_reset();
+    PhaseScope ps;
+    phase_reset(ps);
     P.work = B.cw.ctr;
     // Hybrid: the routing pass also appends the HLL-routed edges to a list
     // (16-byte aligned register rows; else the HLL edges take a second pass
@@ -2112,44 +2707,44 @@ static int run_batch(CountParams P, bool hybrid, const int32_t* vbase, int64_t n
     P.hll_v = hll_list ? B.hw.hll_v : nullptr;
     P.hll_n = hll_list ? B.hw.hll_n : nullptr;
     if (hll_list) TCHLL_CUDA(cudaMemsetAsync(B.hw.hll_n, 0, sizeof(unsigned long long), st));
-    phase_mark(0, st);
-    // pairs with a long table side go to the hub kernel, which publishes
-    // per segment into the graph of x
-    const int hub = hub_threshold(P);
-    if (hybrid) rc = pairs_hist_scan<true>(P, B.cw, hub, st, vbase, n_graphs);
-    else rc = pairs_hist_scan<false>(P, B.cw, hub, st, vbase, n_graphs);
+    phase_mark(ps, 0, st);
+    // pairs with a long table side go to the hub kernels, which publish per
+    // segment into the graph of x
+    const int hub = hub_threshold(P, T);
+    if (hybrid) rc = pairs_hist_scan<true>(P, B.cw, hub, T.hub_seg, st, vbase, n_graphs);
+    else rc = pairs_hist_scan<false>(P, B.cw, hub, T.hub_seg, st, vbase, n_graphs);
     if (rc) return rc;
-    rc = build_chunks(B.cw.off, vbase, n_graphs, P.n_nodes, B, st);  // pair ranges (before the scatter)
+    rc = build_chunks(B.cw.off, vbase, n_graphs, P.n_nodes, B, T.chunk, st);  // pair ranges (before the scatter)
     if (rc) return rc;
     if (hybrid) rc = pairs_scatter<true>(P, B.cw, hub, Q, st);
     else rc = pairs_scatter<false>(P, B.cw, hub, Q, st);
     if (rc) return rc;
-    phase_mark(1, st);
+    phase_mark(ps, 1, st);
     Q.n_edges_dev = nullptr;
     Q.hll_u = nullptr;
-    rc = launch_count<MODE_EXACT>(Q, false, st);
+    rc = launch_count<MODE_EXACT>(Q, T, false, st);
     if (rc) return rc;
     if (hub > 0) {
-        rc = launch_hub(P, B.cw, st, true);
+        rc = launch_hub(P, B.cw, T, ps, st, true);
         if (rc) return rc;
     }
-    phase_mark(2, st);
-    g_phase.used[0] = g_phase.used[1] = true;
+    phase_mark(ps, 2, st);
+    phase_used(ps, 0, 1);
     if (!hybrid) return TCHLL_OK;
     if (hll_list) {  // per-edge estimates into each edge's graph
-        rc = launch_hll_edges(P, B.hw, st);
-        phase_mark(3, st);
-        g_phase.used[2] = true;
+        rc = launch_hll_edges(P, B.hw, T, st);
+        phase_mark(ps, 3, st);
+        phase_used(ps, 2);
         return rc;
     }
     // HLL-routed edges: chunks over each graph's CSR edge range
     TCHLL_CUDA(cudaMemsetAsync(B.cw.ctr + 1, 0, sizeof(unsigned long long), st));
-    rc = build_chunks(P.row_ptr, vbase, n_graphs, P.n_nodes, B, st);
+    rc = build_chunks(P.row_ptr, vbase, n_graphs, P.n_nodes, B, T.chunk, st);
     if (rc) return rc;
     P.work = B.cw.ctr + 1;
-    rc = launch_count<MODE_HYB_HLL>(P, false, st);
-    phase_mark(3, st);
-    g_phase.used[2] = true;
+    rc = launch_count<MODE_HYB_HLL>(P, T, false, st);
+    phase_mark(ps, 3, st);
+    phase_used(ps, 2);
     return rc;
 }
 

@@ -10,20 +10,26 @@
 //                  monotone, so comparing compacted ids gives the same order
 //   CSR            experiment/exp_gpu.py:350-362 (np.lexsort by (src, dst))
 //
-// Pipeline: pack canonical pairs into 63-bit keys -> radix sort -> unique ->
-// endpoint ids sorted + unique (the node table) -> binary-search remap and
-// degree histogram -> orient -> radix sort by (src, dst) -> scan.  Sorting,
-// unique and scans use CUB (header templates compiled into this library); the
-// other passes are kernels written here.
+// Pipeline: largest id (one 16-byte read-back) -> pack canonical pairs into
+// 2k-bit keys, k = bits of the largest id -> radix sort -> unique -> node
+// table and remap -> degree histogram -> orient -> radix sort by (src, dst)
+// packed the same way -> scan.  The node table (compacted id = rank of the
+// raw id among the endpoints) comes from a direct table when the id space
+// fits the workspace (flag every endpoint id, scan the flags: rank[id] is the
+// scan, one gather per endpoint), else from sorting and deduplicating all
+// endpoints and a binary search per endpoint.  Sorting, unique and scans use
+// CUB (header templates compiled into this library); the other passes are
+// kernels written here.
 #include <cub/cub.cuh>
 
 #include "common.cuh"
 
 namespace tchll {
 
-// (2^31-1, 2^31-1) is never a canonical pair (min < max), so it marks dropped
+// Canonical keys are (a << k) | b with a < b < 2^k.  The all-ones key of 2k
+// bits is never a canonical pair (it needs a == b), so it marks dropped
 // self-loops and sorts after every real key.
-constexpr uint64_t kSentinel = (0x7FFFFFFFull << 32) | 0x7FFFFFFFull;
+__host__ __device__ __forceinline__ uint64_t key_sentinel(int k) { return (k >= 32) ? ~0ull : ((1ull << (2 * k)) - 1ull); }
 constexpr uint32_t kEndSentinel = 0xFFFFFFFFu;
 
 struct CsrWs {
@@ -35,7 +41,7 @@ struct CsrWs {
     int32_t* fdeg;
     int32_t* ca;
     int32_t* cb;
-    int64_t* cnt;  // [0] unique keys, [1] unique endpoints, [2] negative-id flag
+    int64_t* cnt;  // [0] unique keys, [1] unique endpoints, [2] negative-id flag, [3] largest id
     void* tmp;
     size_t tmp_bytes;
 };
@@ -84,33 +90,47 @@ static int grid_n(int64_t n, int threads = 256) {
 #define GRID_STRIDE(i, n) \
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
 
-__global__ void canon_kernel(const int32_t* __restrict__ ru, const int32_t* __restrict__ rv, int64_t n,
-                             uint64_t* keys, int64_t* cnt) {
+// Largest endpoint id (atomicMax, one per warp) and the negative-id flag.
+__global__ void max_id_kernel(const int32_t* __restrict__ ru, const int32_t* __restrict__ rv, int64_t n,
+                              int64_t* cnt) {
+    int32_t mx = 0;
     bool neg = false;
     GRID_STRIDE(i, n) {
         const int32_t u = ru[i], v = rv[i];
-        if (u < 0 || v < 0) {
-            neg = true;
-            keys[i] = kSentinel;
-            continue;
-        }
-        const uint32_t a = (uint32_t)(u < v ? u : v), b = (uint32_t)(u < v ? v : u);
-        keys[i] = (u == v) ? kSentinel : (((uint64_t)a << 32) | b);
+        neg |= (u < 0) | (v < 0);
+        mx = max(mx, max(u, v));
     }
-    if (neg) cnt[2] = 1;
+    mx = __reduce_max_sync(0xFFFFFFFFu, mx);
+    neg = __any_sync(0xFFFFFFFFu, neg);
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax((unsigned long long*)(cnt + 3), (unsigned long long)mx);
+        if (neg) cnt[2] = 1;
+    }
+}
+
+__global__ void canon_kernel(const int32_t* __restrict__ ru, const int32_t* __restrict__ rv, int64_t n, int k,
+                             uint64_t* keys) {
+    const uint64_t sent = key_sentinel(k);
+    GRID_STRIDE(i, n) {
+        const int32_t u = ru[i], v = rv[i];
+        const uint32_t a = (uint32_t)(u < v ? u : v), b = (uint32_t)(u < v ? v : u);
+        keys[i] = (u == v || u < 0 || v < 0) ? sent : (((uint64_t)a << k) | b);
+    }
 }
 
 // Endpoints of the unique keys (sentinels become kEndSentinel).
-__global__ void ends_kernel(const uint64_t* __restrict__ keys, int64_t cap, const int64_t* cnt, uint32_t* ends) {
+__global__ void ends_kernel(const uint64_t* __restrict__ keys, int64_t cap, const int64_t* cnt, int kb,
+                            uint32_t* ends) {
     const int64_t nk = cnt[0];
+    const uint64_t sent = key_sentinel(kb), lo = (1ull << kb) - 1ull;
     GRID_STRIDE(i, cap) {
-        uint64_t k = i < nk ? keys[i] : kSentinel;
-        if (k == kSentinel) {
+        uint64_t k = i < nk ? keys[i] : sent;
+        if (k == sent) {
             ends[2 * i] = kEndSentinel;
             ends[2 * i + 1] = kEndSentinel;
         } else {
-            ends[2 * i] = (uint32_t)(k >> 32);
-            ends[2 * i + 1] = (uint32_t)(k & 0xFFFFFFFFu);
+            ends[2 * i] = (uint32_t)(k >> kb);
+            ends[2 * i + 1] = (uint32_t)(k & lo);
         }
     }
 }
@@ -125,24 +145,26 @@ __device__ __forceinline__ int64_t lower_bound_u32(const uint32_t* a, int64_t n,
 }
 
 // Number of real edges / nodes: drop the trailing sentinel when present.
-__device__ __forceinline__ int64_t n_real_edges(const uint64_t* keys, const int64_t* cnt) {
+__device__ __forceinline__ int64_t n_real_edges(const uint64_t* keys, const int64_t* cnt, int kb) {
     const int64_t nk = cnt[0];
-    return (nk > 0 && keys[nk - 1] == kSentinel) ? nk - 1 : nk;
+    return (nk > 0 && keys[nk - 1] == key_sentinel(kb)) ? nk - 1 : nk;
 }
 __device__ __forceinline__ int64_t n_real_nodes(const uint32_t* nodes, const int64_t* cnt) {
     const int64_t nn = cnt[1];
     return (nn > 0 && nodes[nn - 1] == kEndSentinel) ? nn - 1 : nn;
 }
 
+// Sort path: binary search of both endpoints in the sorted node table.
 __global__ void remap_kernel(const uint64_t* __restrict__ keys, int64_t cap, const uint32_t* __restrict__ nodes,
-                             const int64_t* cnt, int32_t* ca, int32_t* cb, int32_t* deg) {
-    const int64_t ne = n_real_edges(keys, cnt);
+                             const int64_t* cnt, int kb, int32_t* ca, int32_t* cb, int32_t* deg) {
+    const int64_t ne = n_real_edges(keys, cnt, kb);
     const int64_t nn = n_real_nodes(nodes, cnt);
+    const uint64_t lo = (1ull << kb) - 1ull;
     GRID_STRIDE(i, cap) {
         if (i >= ne) break;
         const uint64_t k = keys[i];
-        const int32_t a = (int32_t)lower_bound_u32(nodes, nn, (uint32_t)(k >> 32));
-        const int32_t b = (int32_t)lower_bound_u32(nodes, nn, (uint32_t)(k & 0xFFFFFFFFu));
+        const int32_t a = (int32_t)lower_bound_u32(nodes, nn, (uint32_t)(k >> kb));
+        const int32_t b = (int32_t)lower_bound_u32(nodes, nn, (uint32_t)(k & lo));
         ca[i] = a;
         cb[i] = b;
         atomicAdd(deg + a, 1);
@@ -150,34 +172,79 @@ __global__ void remap_kernel(const uint64_t* __restrict__ keys, int64_t cap, con
     }
 }
 
-__global__ void sizes_kernel(const uint64_t* keys, const uint32_t* nodes, const int64_t* cnt, int64_t* sizes) {
+// Direct path: flag[id] = 1 for both endpoints of every unique edge (flag
+// zeroed over [0, max id + 1] before).
+__global__ void flag_ends_kernel(const uint64_t* __restrict__ keys, int64_t cap, const int64_t* cnt, int kb,
+                                 int32_t* flag) {
+    const int64_t ne = n_real_edges(keys, cnt, kb);
+    const uint64_t lo = (1ull << kb) - 1ull;
+    GRID_STRIDE(i, cap) {
+        if (i >= ne) break;
+        const uint64_t k = keys[i];
+        flag[k >> kb] = 1;
+        flag[k & lo] = 1;
+    }
+}
+
+// Direct path, after rank = exclusive scan of flag over [0, ids] (ids = max
+// id + 2 entries): the node table nodes[rank[id]] = id for flagged ids, and
+// the number of nodes in cnt[1] (its sort-path meaning).
+__global__ void rank_nodes_kernel(const int32_t* __restrict__ flag, const int32_t* __restrict__ rank, int64_t ids,
+                                  uint32_t* nodes, int64_t* cnt) {
+    GRID_STRIDE(i, ids) {
+        if (i == ids - 1) cnt[1] = rank[i];  // flag[ids - 1] = 0: the total
+        else if (flag[i]) nodes[rank[i]] = (uint32_t)i;
+    }
+}
+
+// Direct path: both endpoints of every unique edge through the rank table.
+__global__ void remap_direct_kernel(const uint64_t* __restrict__ keys, int64_t cap, const int32_t* __restrict__ rank,
+                                    const int64_t* cnt, int kb, int32_t* ca, int32_t* cb, int32_t* deg) {
+    const int64_t ne = n_real_edges(keys, cnt, kb);
+    const uint64_t lo = (1ull << kb) - 1ull;
+    GRID_STRIDE(i, cap) {
+        if (i >= ne) break;
+        const uint64_t k = keys[i];
+        const int32_t a = __ldg(rank + (k >> kb)), b = __ldg(rank + (k & lo));
+        ca[i] = a;
+        cb[i] = b;
+        atomicAdd(deg + a, 1);
+        atomicAdd(deg + b, 1);
+    }
+}
+
+__global__ void sizes_kernel(const uint64_t* keys, const uint32_t* nodes, const int64_t* cnt, int kb, int direct,
+                             int64_t* sizes) {
     if (cnt[2]) {
         sizes[0] = -1;
         sizes[1] = -1;
         return;
     }
-    sizes[0] = n_real_nodes(nodes, cnt);
-    sizes[1] = n_real_edges(keys, cnt);
+    sizes[0] = direct ? cnt[1] : n_real_nodes(nodes, cnt);
+    sizes[1] = n_real_edges(keys, cnt, kb);
 }
 
+// Orientation u -> v iff (deg u, u) < (deg v, v); oriented keys (s << kn) | d
+// with kn = bits of the largest compacted id.
 __global__ void orient_kernel(const int32_t* __restrict__ ca, const int32_t* __restrict__ cb, int64_t ne,
-                              const int32_t* __restrict__ deg, int32_t* fdeg, uint64_t* okeys) {
+                              const int32_t* __restrict__ deg, int kn, int32_t* fdeg, uint64_t* okeys) {
     GRID_STRIDE(i, ne) {
         const int32_t a = ca[i], b = cb[i];
         const int32_t da = deg[a], db = deg[b];
         const bool first = (da < db) || (da == db && a < b);
         const int32_t s = first ? a : b, d = first ? b : a;
         atomicAdd(fdeg + s, 1);
-        okeys[i] = ((uint64_t)(uint32_t)s << 32) | (uint32_t)d;
+        okeys[i] = ((uint64_t)(uint32_t)s << kn) | (uint32_t)d;
     }
 }
 
-__global__ void split_kernel(const uint64_t* __restrict__ okeys, int64_t ne, int32_t* col_idx, int32_t* edge_u,
-                             int32_t* edge_v) {
+__global__ void split_kernel(const uint64_t* __restrict__ okeys, int64_t ne, int kn, int32_t* col_idx,
+                             int32_t* edge_u, int32_t* edge_v) {
+    const uint64_t lo = (1ull << kn) - 1ull;
     GRID_STRIDE(i, ne) {
         const uint64_t k = okeys[i];
-        const int32_t d = (int32_t)(k & 0xFFFFFFFFu);
-        edge_u[i] = (int32_t)(k >> 32);
+        const int32_t d = (int32_t)(k & lo);
+        edge_u[i] = (int32_t)(k >> kn);
         col_idx[i] = d;
         edge_v[i] = d;
     }
@@ -282,25 +349,57 @@ TCHLL_EXPORT int tchll_csr_build_phase1(const int32_t* raw_u, const int32_t* raw
         TCHLL_CUDA(cudaMemsetAsync(sizes, 0, 2 * sizeof(int64_t), st));
         return TCHLL_OK;
     }
-    canon_kernel<<<grid_n(n_raw), 256, 0, st>>>(raw_u, raw_v, n_raw, W.k0, W.cnt);
+    // the largest id sizes the keys and picks the node-table method: one
+    // 16-byte read-back (the stream is waited for here)
+    max_id_kernel<<<grid_n(n_raw), 256, 0, st>>>(raw_u, raw_v, n_raw, W.cnt);
+    TCHLL_CHECK_LAUNCH("max_id_kernel");
+    int64_t hc[2] = {0, 0};
+    TCHLL_CUDA(cudaMemcpyAsync(hc, W.cnt + 2, sizeof(hc), cudaMemcpyDeviceToHost, st));
+    TCHLL_CUDA(cudaStreamSynchronize(st));
+    if (hc[0]) {  // a negative id: sizes -1, nothing else
+        sizes_kernel<<<1, 1, 0, st>>>(W.k0, W.e0, W.cnt, 1, 0, sizes);
+        TCHLL_CHECK_LAUNCH("sizes_kernel");
+        return TCHLL_OK;
+    }
+    const int64_t max_id = hc[1];
+    const int kb = bits_for(max_id);
+    canon_kernel<<<grid_n(n_raw), 256, 0, st>>>(raw_u, raw_v, n_raw, kb, W.k0);
     TCHLL_CHECK_LAUNCH("canon_kernel");
     size_t tb = W.tmp_bytes;
-    TCHLL_CUDA(cub::DeviceRadixSort::SortKeys(W.tmp, tb, W.k0, W.k1, R, 0, 63, st));
+    TCHLL_CUDA(cub::DeviceRadixSort::SortKeys(W.tmp, tb, W.k0, W.k1, R, 0, 2 * kb, st));
     count_launch();
     tb = W.tmp_bytes;
     TCHLL_CUDA(cub::DeviceSelect::Unique(W.tmp, tb, W.k1, W.k0, W.cnt + 0, R, st));
     count_launch();
-    ends_kernel<<<grid_n(n_raw), 256, 0, st>>>(W.k0, n_raw, W.cnt, W.e0);
-    TCHLL_CHECK_LAUNCH("ends_kernel");
-    tb = W.tmp_bytes;
-    TCHLL_CUDA(cub::DeviceRadixSort::SortKeys(W.tmp, tb, W.e0, W.e1, 2 * R, 0, 32, st));
-    count_launch();
-    tb = W.tmp_bytes;
-    TCHLL_CUDA(cub::DeviceSelect::Unique(W.tmp, tb, W.e1, W.e0, W.cnt + 1, 2 * R, st));
-    count_launch();
-    remap_kernel<<<grid_n(n_raw), 256, 0, st>>>(W.k0, n_raw, W.e0, W.cnt, W.ca, W.cb, W.deg);
-    TCHLL_CHECK_LAUNCH("remap_kernel");
-    sizes_kernel<<<1, 1, 0, st>>>(W.k0, W.e0, W.cnt, sizes);
+    // direct rank table when ids 0 .. max_id (+ a zero flag) fit the 2R-entry
+    // endpoint buffers, else sort and deduplicate the endpoints
+    const int64_t ids = max_id + 2;
+    const int direct = ids <= 2 * (int64_t)R ? 1 : 0;
+    if (direct) {
+        TCHLL_CUDA(cudaMemsetAsync(W.fdeg, 0, (size_t)ids * sizeof(int32_t), st));
+        flag_ends_kernel<<<grid_n(n_raw), 256, 0, st>>>(W.k0, n_raw, W.cnt, kb, W.fdeg);
+        TCHLL_CHECK_LAUNCH("flag_ends_kernel");
+        int32_t* rank = reinterpret_cast<int32_t*>(W.e1);
+        tb = W.tmp_bytes;
+        TCHLL_CUDA(cub::DeviceScan::ExclusiveSum(W.tmp, tb, W.fdeg, rank, (int)ids, st));
+        count_launch();
+        rank_nodes_kernel<<<grid_n(ids), 256, 0, st>>>(W.fdeg, rank, ids, W.e0, W.cnt);
+        TCHLL_CHECK_LAUNCH("rank_nodes_kernel");
+        remap_direct_kernel<<<grid_n(n_raw), 256, 0, st>>>(W.k0, n_raw, rank, W.cnt, kb, W.ca, W.cb, W.deg);
+        TCHLL_CHECK_LAUNCH("remap_direct_kernel");
+    } else {
+        ends_kernel<<<grid_n(n_raw), 256, 0, st>>>(W.k0, n_raw, W.cnt, kb, W.e0);
+        TCHLL_CHECK_LAUNCH("ends_kernel");
+        tb = W.tmp_bytes;
+        TCHLL_CUDA(cub::DeviceRadixSort::SortKeys(W.tmp, tb, W.e0, W.e1, 2 * R, 0, 32, st));
+        count_launch();
+        tb = W.tmp_bytes;
+        TCHLL_CUDA(cub::DeviceSelect::Unique(W.tmp, tb, W.e1, W.e0, W.cnt + 1, 2 * R, st));
+        count_launch();
+        remap_kernel<<<grid_n(n_raw), 256, 0, st>>>(W.k0, n_raw, W.e0, W.cnt, kb, W.ca, W.cb, W.deg);
+        TCHLL_CHECK_LAUNCH("remap_kernel");
+    }
+    sizes_kernel<<<1, 1, 0, st>>>(W.k0, W.e0, W.cnt, kb, direct, sizes);
     TCHLL_CHECK_LAUNCH("sizes_kernel");
     return TCHLL_OK;
 }
@@ -322,13 +421,13 @@ TCHLL_EXPORT int tchll_csr_build_phase2(int64_t n_raw, int64_t n_nodes, int64_t 
     cudaStream_t st = (cudaStream_t)stream;
     TCHLL_CUDA(cudaMemsetAsync(W.fdeg, 0, ((size_t)n_nodes + 1) * sizeof(int32_t), st));
     if (n_edges > 0) {
-        orient_kernel<<<grid_n(n_edges), 256, 0, st>>>(W.ca, W.cb, n_edges, W.deg, W.fdeg, W.k1);
+        const int kn = bits_for(n_nodes > 1 ? n_nodes - 1 : 1);
+        orient_kernel<<<grid_n(n_edges), 256, 0, st>>>(W.ca, W.cb, n_edges, W.deg, kn, W.fdeg, W.k1);
         TCHLL_CHECK_LAUNCH("orient_kernel");
         size_t tb = W.tmp_bytes;
-        const int end_bit = 32 + bits_for(n_nodes > 1 ? n_nodes - 1 : 1);
-        TCHLL_CUDA(cub::DeviceRadixSort::SortKeys(W.tmp, tb, W.k1, W.k0, (int)n_edges, 0, end_bit, st));
+        TCHLL_CUDA(cub::DeviceRadixSort::SortKeys(W.tmp, tb, W.k1, W.k0, (int)n_edges, 0, 2 * kn, st));
         count_launch();
-        split_kernel<<<grid_n(n_edges), 256, 0, st>>>(W.k0, n_edges, col_idx, edge_u, edge_v);
+        split_kernel<<<grid_n(n_edges), 256, 0, st>>>(W.k0, n_edges, kn, col_idx, edge_u, edge_v);
         TCHLL_CHECK_LAUNCH("split_kernel");
     }
     size_t tb = W.tmp_bytes;

@@ -107,6 +107,26 @@ def sharded_count(n_edges: int, costs: np.ndarray, count_range: Callable[[int, i
     return combine(gather_results(local, group))
 
 
+class ShardedExact:
+    """One rank's part of an exact count split by edges: the rank's
+    contiguous, cost-balanced edge range, counted with ``count_range(lo, hi)``
+    (the libtchll kernels on a GPU, any counter of the same shape in a test),
+    then one all_gather of the 64-byte result blocks and the exact integer
+    combination.  ``step()`` returns the whole graph's count on every rank.
+    Collective: every rank calls step() the same number of times."""
+
+    def __init__(self, costs, count_range: Callable[[int, int], Tuple[int, ...]], group=None):
+        self.group = group
+        rank = dist.get_rank(group)
+        world = dist.get_world_size(group)
+        self.lo, self.hi = shard_bounds(costs, world)[rank]
+        self.count_range = count_range
+
+    def step(self) -> dict:
+        local = self.count_range(self.lo, self.hi)
+        return combine(gather_results(local, self.group))
+
+
 def gpu_exact_range(g) -> Callable[[int, int], Tuple[int, ...]]:
     """count_range for the exact count on a device CSR (libtchll kernels)."""
     from . import core

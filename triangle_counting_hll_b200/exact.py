@@ -9,9 +9,13 @@ intersection method per edge group on its own, with identical counts.
 
 With ``per_edge_timing=True`` the per-edge records ``(u, v, deg_u, deg_v,
 support, time_s)`` come in the reference's order (dict order, skipping edges
-whose lists are empty, src/exact.py:79-91); ``support`` is exact and
-``time_s`` is the measured device time divided evenly over the recorded edges
-(a single launch has no per-edge clock).
+whose lists are empty, src/exact.py:79-91); ``support`` is exact.  ``time_s``
+differs from the reference's: the reference clocks each intersection on the
+host (src/exact.py:86-90), while here all edges are counted by one device
+launch, which has no per-edge clock.  Each edge's ``time_s`` is the call's
+measured time apportioned by the edge's probe count, min(deg_u, deg_v) + 1
+(the kernel probes the shorter list into a table of the longer one), so the
+records sum to ``elapsed`` and rank edges by their real cost.
 """
 from __future__ import annotations
 
@@ -68,7 +72,10 @@ def exact_triangle_count(forward_adj: Dict[int, np.ndarray], r: float = 8.0,
                          per_edge_timing: bool = False) -> Tuple[int, float, List]:
     """T = sum over oriented edges (u, v) of |N+(u) cap N+(v)|.
 
-    Returns ``(count, elapsed_s, edge_data)`` (src/exact.py:48-98)."""
+    Returns ``(count, elapsed_s, edge_data)`` (src/exact.py:48-98).  With
+    per_edge_timing, edge_data holds ``(u, v, deg_u, deg_v, support, time_s)``
+    per edge; time_s is modelled, not clocked: the call's elapsed time split
+    in proportion to min(deg_u, deg_v) + 1, the edge's probe count."""
     _lib.require_cuda()
     adj = core.adjacency_with_missing_nodes(forward_adj)
     g = adj.csr
@@ -101,5 +108,7 @@ def _edge_records(forward_adj, adj: core.AdjacencyCSR, support_csr: np.ndarray, 
             if lens[j] == 0:
                 continue
             recs.append([u, int(v), len(nbrs_u), int(lens[j]), int(support_csr[base + k])])
-    per = elapsed / len(recs) if recs else 0.0
-    return [tuple(x + [per]) for x in recs]
+    # the launch's time apportioned by each edge's probe count
+    w = np.array([min(x[2], x[3]) + 1 for x in recs], dtype=np.float64)
+    share = (elapsed * w / w.sum()) if recs else w
+    return [tuple(x + [float(t)]) for x, t in zip(recs, share)]

@@ -10,13 +10,16 @@ The reference answers one query per call, synchronously (src/gpu_hybrid.py:
   resident; least-recently-used resident graphs are evicted to make room, and
   a request that could never fit is completed with an error;
 * graphs stay resident after their query, so repeat queries skip the build;
-* every tick, the newly admitted graphs are built on a build stream while
+  a query for a graph still being built waits for that build;
+* admitted graphs are built by a worker thread on a build stream while
   earlier counts run on a count stream, so arrivals overlap with work
-  already on the device: small graphs are counted together (one batched
-  count launch per mode, exact and hybrid, over their concatenated CSRs),
-  large graphs (at least ``big_edges`` raw edges, which fill the GPU on their
-  own) one at a time, each count launched as soon as its graph is built;
-  finished counts are answered as the host sees them.
+  already on the device and the serving loop itself never waits for the
+  GPU (the CSR build's size read-back blocks the worker only): small graphs
+  are built and counted together (one batched count launch per mode, exact
+  and hybrid, over their concatenated CSRs), large graphs (at least
+  ``big_edges`` raw edges, which fill the GPU on their own) one at a time,
+  each count launched as soon as its build is seen finished; finished
+  counts are polled and answered as the host sees them.
   Per-graph results are bit-identical to answering each query alone;
 * latency is completion time minus arrival time; the report gives p50 / p99
   and graphs/s next to the same requests served one at a time.
@@ -25,6 +28,8 @@ from __future__ import annotations
 
 import collections
 import math
+import queue
+import threading
 import time
 from dataclasses import dataclass, field
 from typing import Dict, List, Optional, Sequence, Tuple
@@ -154,7 +159,59 @@ def _server_streams(dev: torch.device) -> Tuple[torch.cuda.Stream, torch.cuda.St
     return _STREAMS[idx]
 
 
+class _BuildWorker(threading.Thread):
+    """Builds graphs (device generator, CSR build, compact sketches of large
+    hybrid queries) on the server's build stream, off the serving loop: the
+    CSR build reads its vertex and edge counts back to size its outputs, and
+    those waits block this thread only.  Each finished job comes back with
+    an event recorded on the build stream after it."""
+
+    def __init__(self, dev, build_stream, big_edges: int):
+        super().__init__(daemon=True)
+        self.dev = dev
+        self.stream = build_stream
+        self.big_edges = big_edges
+        self.inbox: "queue.Queue" = queue.Queue()
+        self.outbox: "queue.Queue" = queue.Queue()
+
+    def run(self):
+        torch.cuda.set_device(self.dev)
+        while True:
+            job = self.inbox.get()
+            if job is None:
+                return
+            out, exc = [], None
+            try:
+                with torch.cuda.stream(self.stream):
+                    for key, req, csr in job:
+                        if csr is None:  # a new graph
+                            u, v = generate_edges(req, self.dev)
+                            csr = core.csr_from_edges(u, v, device=self.dev)
+                            del u, v
+                            sk = None
+                            if req.mode == "hybrid" and csr.n_edges >= self.big_edges:
+                                sk = _compact_sketches(csr, req)
+                            out.append((key, csr, sk))
+                        else:  # sketches of a resident large graph
+                            out.append((key, None, _compact_sketches(csr, req)))
+                    ev = torch.cuda.Event()
+                    ev.record(self.stream)
+            except Exception as e:  # reported with the job's queries
+                exc, ev = e, None
+            self.outbox.put((job, out, ev, exc))
+
+
+def _compact_sketches(csr: core.DeviceCSR, req: Request):
+    slot, n_rows = core.sketch_slots(csr.row_ptr, req.theta)
+    rows = core.build_sketches_compact_tensors(csr.row_ptr, csr.col_idx, slot, n_rows, req.p)
+    return (req.p, req.theta), (rows, slot)
+
+
 class Server:
+    """Continuous-batching server on one GPU: a serving loop (admission,
+    count launches, answers) plus a build worker thread.  See the module
+    docstring."""
+
     def __init__(self, device=None, budget_bytes: float = 120e9, max_batch: int = 256,
                  max_batch_edges: float = 4e8, big_edges: int = 1 << 20):
         self.dev = core._device(device)
@@ -164,18 +221,21 @@ class Server:
         self.max_batch_edges = int(max_batch_edges)
         self.resident: "collections.OrderedDict[Tuple, Resident]" = collections.OrderedDict()
         self.resident_bytes = 0
+        self.inflight_bytes = 0  # admission estimates of the jobs in the build worker
         self.build_stream, self.count_stream = _server_streams(self.dev)
         self.stats = {"ticks": 0, "built": 0, "cache_hits": 0, "evicted": 0, "rejected": 0, "batch_sizes": [],
                       "single_launches": 0, "batched_launches": 0}
         self.busy: set = set()  # keys whose graphs the in-flight launches read
+        self.building: Dict[Tuple, List[Request]] = {}  # keys in the build worker -> queries waiting on them
         self.pending: list = []  # launched, unanswered: (mode, requests, results, event, buffers)
         self._done: List[Completion] = []
         self._t0 = 0.0
 
     # ----------------------------------------------------------- memory
     def _evict_for(self, need: int, pinned: set) -> bool:
-        while self.resident_bytes + need > self.budget:
-            victim = next((k for k in self.resident if k not in pinned and k not in self.busy), None)
+        while self.resident_bytes + self.inflight_bytes + need > self.budget:
+            victim = next((k for k in self.resident
+                           if k not in pinned and k not in self.busy and k not in self.building), None)
             if victim is None:
                 return False
             r = self.resident.pop(victim)
@@ -184,82 +244,119 @@ class Server:
         return True
 
     # ------------------------------------------------------------ stages
-    def _admit(self, queue: "collections.deque[Request]", done: List[Completion], now: float) -> List[Request]:
-        """FIFO admission under the byte budget and batch limits."""
-        taken: List[Request] = []
+    def _admit(self, queue_: "collections.deque[Request]", done: List[Completion], now: float):
+        """FIFO admission under the byte budget and batch limits.  Returns
+        (queries whose graphs are resident, build jobs for the worker)."""
+        ready: List[Request] = []
+        small_job: list = []
+        jobs: list = []
         pinned: set = set()
-        reserve = 0
         edges = 0
-        while queue and len(taken) < self.max_batch:
-            r = queue[0]
-            if r.key in self.resident:  # sketches of a resident graph may still be missing
-                res = self.resident[r.key]
-                need = sketch_bytes(r) if (r.mode == "hybrid" and res.csr.n_edges >= self.big_edges
-                                           and (r.p, r.theta) not in res.sketches) else 0
-            else:
-                need = estimate_bytes(r)
+        taken = 0
+        while queue_ and taken < self.max_batch:
+            r = queue_[0]
+            if r.key in self.building:  # its graph is being built: answer it with that build
+                queue_.popleft()
+                self.building[r.key].append(r)
+                taken += 1
+                continue
+            res = self.resident.get(r.key)
+            if res is not None:
+                if r.mode == "hybrid" and res.csr.n_edges >= self.big_edges and (r.p, r.theta) not in res.sketches:
+                    need = sketch_bytes(r)
+                    if not self._evict_for(need, pinned | {r.key}):
+                        break
+                    queue_.popleft()
+                    self.building[r.key] = [r]
+                    self.inflight_bytes += need
+                    jobs.append([(r.key, r, res.csr)])
+                else:
+                    queue_.popleft()
+                    ready.append(r)
+                    self.stats["cache_hits"] += 1
+                pinned.add(r.key)
+                taken += 1
+                continue
+            need = estimate_bytes(r)
             if need > self.budget:
-                queue.popleft()
+                queue_.popleft()
                 self.stats["rejected"] += 1
                 done.append(Completion(r.rid, r.mode, None, latency=now - r.arrival,
                                        error=f"needs ~{need / 1e9:.1f} GB, over the {self.budget / 1e9:.1f} GB budget"))
                 continue
-            if taken and (edges + r.raw_edges() > self.max_batch_edges):
+            if taken and edges + r.raw_edges() > self.max_batch_edges:
                 break
-            if not self._evict_for(reserve + need, pinned | {q.key for q in taken}):
+            if not self._evict_for(need, pinned):
                 break
-            queue.popleft()
-            taken.append(r)
-            pinned.add(r.key)
-            reserve += need
-            edges += r.raw_edges()
-        return taken
-
-    def _build(self, reqs: List[Request]) -> None:
-        """Build the graphs of reqs that are not resident (device CSR builds
-        on the build stream), and make them resident."""
-        todo: Dict[Tuple, Request] = {}
-        for r in reqs:
-            if r.key in self.resident:
-                self.stats["cache_hits"] += 1
+            queue_.popleft()
+            self.building[r.key] = [r]
+            self.inflight_bytes += need
+            self._est[r.key] = need
+            if r.raw_edges() < self.big_edges:
+                small_job.append((r.key, r, None))
             else:
-                todo.setdefault(r.key, r)
-        if not todo:
-            return
-        built = []
-        with torch.cuda.stream(self.build_stream):
-            for kr in todo.items():
-                u, v = generate_edges(kr[1], self.dev)
-                built.append((kr, core.csr_from_edges(u, v, device=self.dev)))
-                del u, v
-        for (key, r), csr in built:
-            nb = csr.nbytes()
-            self.resident[key] = Resident(csr, nb)
-            self.resident_bytes += nb
-            self.stats["built"] += 1
+                jobs.append([(r.key, r, None)])
+            edges += r.raw_edges()
+            taken += 1
+        if small_job:  # small graphs: one job, then one batched launch
+            jobs.insert(0, small_job)
+        for job in jobs:
+            for key, r, csr in job:
+                if csr is not None:
+                    self._est[key] = sketch_bytes(r)
+            self._worker.inbox.put(job)
+        if taken:
+            self.stats["ticks"] += 1
+            self.stats["batch_sizes"].append(taken)
+        return ready
 
-    def _sketch(self, reqs: List[Request]) -> None:
-        """Compact sketches of the large graphs of hybrid queries, on the build
-        stream (their row count is read back here, not in the launch stage,
-        so the count stream is never waited on while launching)."""
-        with torch.cuda.stream(self.build_stream):
-            for r in reqs:
-                res = self.resident[r.key]
-                if r.mode != "hybrid" or res.csr.n_edges < self.big_edges or (r.p, r.theta) in res.sketches:
-                    continue
-                g = res.csr
-                slot, n_rows = core.sketch_slots(g.row_ptr, r.theta)
-                rows = core.build_sketches_compact_tensors(g.row_ptr, g.col_idx, slot, n_rows, r.p)
-                res.sketches[(r.p, r.theta)] = (rows, slot)
-                nb = rows.numel() + slot.numel() * slot.element_size()
-                res.nbytes += nb
-                self.resident_bytes += nb
+    def _collect(self) -> bool:
+        """Make the worker's finished builds resident and launch the queries
+        waiting on them; returns whether anything finished."""
+        got = False
+        while True:
+            try:
+                job, out, ev, exc = self._worker.outbox.get_nowait()
+            except queue.Empty:
+                return got
+            got = True
+            now = time.perf_counter() - self._t0
+            for key, _, _ in job:
+                self.inflight_bytes -= self._est.pop(key, 0)
+            if exc is not None:
+                for key, _, _ in job:
+                    for r in self.building.pop(key, []):
+                        self._done.append(Completion(r.rid, r.mode, None, latency=now - r.arrival,
+                                                     error=f"build failed: {exc}"))
+                continue
+            self.count_stream.wait_event(ev)
+            waiting: List[Request] = []
+            for key, csr, sk in out:
+                if csr is not None:
+                    self.resident[key] = Resident(csr, csr.nbytes())
+                    self.resident_bytes += self.resident[key].nbytes
+                    self.stats["built"] += 1
+                res = self.resident[key]
+                if sk is not None:
+                    (pt, (rows, slot)) = sk
+                    res.sketches[pt] = (rows, slot)
+                    nb = rows.numel() + slot.numel() * slot.element_size()
+                    res.nbytes += nb
+                    self.resident_bytes += nb
+                waiting += self.building.pop(key, [])
+            self._launch_all(waiting)
+
+    def _launch_all(self, reqs: List[Request]) -> None:
+        if not reqs:
+            return
+        self.pending += self._launch(reqs)
+        self.busy = {r.key for it in self.pending for r in it[1]}
 
     def _launch(self, reqs: List[Request]):
-        """Fold the tick's queries into one batched launch per mode on the
-        count stream; returns what is needed to finish them."""
+        """Fold queries on resident graphs into one batched launch per mode on
+        the count stream (large graphs, and a lone query, one launch each);
+        returns what is needed to finish them."""
         pending = []
-        self.count_stream.wait_stream(self.build_stream)
         with torch.cuda.stream(self.count_stream):
             for mode in ("exact", "hybrid"):
                 group = [r for r in reqs if r.mode == mode]
@@ -270,14 +367,12 @@ class Server:
                     for t in (c.row_ptr, c.col_idx, c.degrees, c.node_ids, c.edge_u, c.edge_v):
                         t.record_stream(self.count_stream)
                 r0 = group[0]  # one (p, theta, gamma) per launch; the workload uses one setting
-                # large graphs, and a lone query, run the single-graph path
-                # (same kernels and integer totals, no concatenation)
                 lone = [i for i, g in enumerate(csrs) if len(group) == 1 or g.n_edges >= self.big_edges]
                 lone_set = set(lone)
                 rest = [i for i in range(len(group)) if i not in lone_set]
-                keep = []
                 for i in lone:
                     g = csrs[i]
+                    keep = []
                     res = torch.empty(_lib.RESULT_BYTES, dtype=torch.uint8, device=self.dev)
                     if mode == "exact":
                         core.exact_count_tensors(g.row_ptr, g.col_idx, g.edge_u, g.edge_v, result=res)
@@ -333,57 +428,56 @@ class Server:
             for r in group:
                 done.append(Completion(r.rid, mode, None, latency=now - r.arrival, error=str(exc)))
 
-    def _reap(self, block: bool = False) -> None:
-        """Answer every launched query whose count has finished (the oldest
-        one first, waiting for it when block is set); a query's latency ends
-        when the host sees its result."""
+    def _reap(self) -> bool:
+        """Answer every launched query whose count has finished, never
+        waiting; a query's latency ends when the host sees its result.
+        Returns whether anything was answered."""
         keep = []
-        for k, item in enumerate(self.pending):
-            if block and k == 0:
-                item[3].synchronize()
-            if not keep and item[3].query():
+        got = False
+        for item in self.pending:
+            if not keep and item[3].query():  # the count stream finishes launches in order
                 self._complete(item, self._done, self._t0)
+                got = True
             else:
-                keep.append(item)  # the count stream finishes launches in order
+                keep.append(item)
         self.pending = keep
         self.busy = {r.key for it in self.pending for r in it[1]}
+        return got
 
     # -------------------------------------------------------------- loop
     def serve(self, requests: Sequence[Request]) -> List[Completion]:
         """Serve requests in real time (arrival = seconds after the call);
-        returns one Completion per request, ordered by request id.  Launches
-        of several ticks may be in flight on the count stream at once."""
+        returns one Completion per request, ordered by request id.  The loop
+        never waits for the GPU: builds run in the worker thread, counts of
+        several ticks may be in flight on the count stream, and finished
+        counts are polled."""
         reqs = sorted(requests, key=lambda r: r.arrival)
-        queue: "collections.deque[Request]" = collections.deque()
-        self._done: List[Completion] = []
-        self._t0 = t0 = time.perf_counter()
+        queue_: "collections.deque[Request]" = collections.deque()
+        self._done = []
+        self._est: Dict[Tuple, int] = {}
         self.pending = []
+        self._worker = _BuildWorker(self.dev, self.build_stream, self.big_edges)
+        self._worker.start()
+        self._t0 = t0 = time.perf_counter()
         i = 0
-        while len(self._done) < len(reqs):
-            now = time.perf_counter() - t0
-            while i < len(reqs) and reqs[i].arrival <= now:
-                queue.append(reqs[i])
-                i += 1
-            self._reap()
-            nxt = self._admit(queue, self._done, now) if queue else []
-            if nxt:
-                self.stats["ticks"] += 1
-                self.stats["batch_sizes"].append(len(nxt))
-                # small graphs: one batched build and launch; large graphs:
-                # each built and launched in turn, so its count runs while
-                # the host builds the next one
-                small = [r for r in nxt if r.raw_edges() < self.big_edges]
-                stages = ([small] if small else []) + [[r] for r in nxt if r.raw_edges() >= self.big_edges]
-                for part in stages:
-                    self._build(part)         # overlaps with the in-flight counts
-                    self._sketch(part)
-                    self.pending += self._launch(part)
-                    self.busy = {r.key for it in self.pending for r in it[1]}
-                    self._reap()
-            elif self.pending:
-                self._reap(block=True)
-            elif not queue and i < len(reqs):
-                time.sleep(max(0.0, min(reqs[i].arrival - (time.perf_counter() - t0), 0.002)))
+        try:
+            while len(self._done) < len(reqs):
+                now = time.perf_counter() - t0
+                while i < len(reqs) and reqs[i].arrival <= now:
+                    queue_.append(reqs[i])
+                    i += 1
+                busy = self._reap()
+                busy |= self._collect()
+                ready = self._admit(queue_, self._done, now) if queue_ else []
+                if ready:
+                    self._launch_all(ready)
+                    busy = True
+                if not busy:  # nothing to do until an arrival, a build or a count finishes
+                    nxt = reqs[i].arrival - (time.perf_counter() - t0) if i < len(reqs) else 1.0
+                    time.sleep(max(0.0, min(nxt, 0.0002)))
+        finally:
+            self._worker.inbox.put(None)
+            self._worker.join(timeout=60)
         return sorted(self._done, key=lambda c: c.rid)
 
 
@@ -431,39 +525,67 @@ def latency_summary(done: Sequence[Completion], wall_s: float) -> Dict:
             "graphs_per_s": len(ok) / wall_s if wall_s > 0 else None}
 
 
-def bench_entry(dev, quick: bool = True) -> Dict:
-    """Serving workload at several Poisson rates: p50/p99 latency and
-    graphs/s of the continuous-batching server versus answering the same
-    requests one at a time; results checked identical between the two."""
-    n = 300 if quick else 20000
-    out: Dict = {"requests_per_rate": n, "workload": "R-MAT scale U[12,20], ef U[8,32], 50/50 exact / hybrid "
-                 "(p=12, theta=gamma=128), Poisson arrivals, 120 GB admission budget"}
-    # warm both paths (allocator pools of the server streams and the default
-    # stream, lazy kernel loading) on requests outside the timed sets
+def _warm(dev) -> None:
+    """Warm both paths (allocator pools of the server streams and the default
+    stream, lazy kernel loading) on requests outside the timed sets, then one
+    paced run like the timed ones, so the server's streams have served
+    requests arriving one at a time too."""
     warm = [Request(i, 0.0, 20, 32, 777 + i, m) for i, m in enumerate(("exact", "hybrid", "exact", "hybrid"))]
     warm += c5_requests(40, 1e6, seed=12345)
     for _ in range(2):
         Server(dev, budget_bytes=120e9).serve(warm)
         serve_sequential(warm, dev)
-    # and one paced run like the timed ones (other graphs), so the server's
-    # streams have served requests arriving one at a time too
     Server(dev, budget_bytes=120e9).serve(c5_requests(60, 50.0, seed=4242))
     torch.cuda.synchronize(dev)
+
+
+def _compare(dev, reqs) -> Dict:
+    srv = Server(dev, budget_bytes=120e9)
+    t0 = time.perf_counter()
+    got = srv.serve(reqs)
+    wall = time.perf_counter() - t0
+    s = latency_summary(got, wall)
+    s["mean_batch"] = float(np.mean(srv.stats["batch_sizes"])) if srv.stats["batch_sizes"] else 0.0
+    s["builds"] = srv.stats["built"]
+    s["batched_launches"] = srv.stats["batched_launches"]
+    s["single_launches"] = srv.stats["single_launches"]
+    del srv
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    ref = serve_sequential(reqs, dev)
+    wall_p = time.perf_counter() - t0
+    sp = latency_summary(ref, wall_p)
+    same = all(a.value == b.value and a.stats == b.stats for a, b in zip(got, ref))
+    return {"requests": len(reqs), "server": s, "sequential": sp, "identical_results": same,
+            "throughput_ratio": (s["graphs_per_s"] or 0) / max(sp["graphs_per_s"] or 1e-9, 1e-9),
+            "p99_ratio": (s["p99_ms"] or 0) / max(sp["p99_ms"] or 1e-9, 1e-9)}
+
+
+def bench_entry(dev, quick: bool = True) -> Dict:
+    """Serving workload at several Poisson rates: p50/p99 latency and
+    graphs/s of the continuous-batching server versus answering the same
+    requests one at a time; results checked identical between the two.
+    (The quick form, 300 requests per rate, for the headline line; bench_c5
+    runs the full 20,000.)"""
+    n = 300 if quick else 20000
+    out: Dict = {"requests_per_rate": n, "workload": "R-MAT scale U[12,20], ef U[8,32], 50/50 exact / hybrid "
+                 "(p=12, theta=gamma=128), Poisson arrivals, 120 GB admission budget"}
+    _warm(dev)
     for rate in (50.0, 200.0, 1000.0):
-        reqs = c5_requests(n, rate, seed=int(rate))
-        srv = Server(dev, budget_bytes=120e9)
-        t0 = time.perf_counter()
-        got = srv.serve(reqs)
-        wall = time.perf_counter() - t0
-        s = latency_summary(got, wall)
-        s["mean_batch"] = float(np.mean(srv.stats["batch_sizes"])) if srv.stats["batch_sizes"] else 0.0
-        torch.cuda.synchronize(dev)
-        t0 = time.perf_counter()
-        ref = serve_sequential(reqs, dev)
-        wall_p = time.perf_counter() - t0
-        sp = latency_summary(ref, wall_p)
-        same = all(a.value == b.value and a.stats == b.stats for a, b in zip(got, ref))
-        out[f"rate_{int(rate)}"] = {"server": s, "sequential": sp, "identical_results": same,
-                                    "throughput_ratio": (s["graphs_per_s"] or 0) / max(sp["graphs_per_s"] or 1e-9,
-                                                                                       1e-9)}
+        out[f"rate_{int(rate)}"] = _compare(dev, c5_requests(n, rate, seed=int(rate)))
+    return out
+
+
+def bench_c5(dev, n_saturating: int = 20000, rates=((2000.0, 20000), (400.0, 4000), (100.0, 1500))) -> Dict:
+    """The serving configuration at full size: 20,000 requests arriving
+    faster than either path can serve them (2,000/s), plus lower Poisson
+    rates with the request counts given (about 10-15 s of arrivals each),
+    each against the same requests served one at a time."""
+    out: Dict = {"workload": "R-MAT scale U[12,20], ef U[8,32], 50/50 exact / hybrid (p=12, theta=gamma=128), "
+                             "Poisson arrivals, 120 GB admission budget"}
+    _warm(dev)
+    for rate, n in rates:
+        if rate == rates[0][0]:
+            n = n_saturating
+        out[f"rate_{int(rate)}"] = _compare(dev, c5_requests(n, rate, seed=int(rate)))
     return out
