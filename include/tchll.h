@@ -159,25 +159,27 @@ int tchll_get_count_hub(int32_t* out4 /* host */);
 
 /* Hub core (pairs layout, with the padded lists in the workspace): the hub
  * kernels work in the coordinates of the core, the vertices that appear in
- * some hub table side's forward list, and probe only the core members of
- * each probe list; when the core fits 8 * 2^bitmap_log2 bits of shared
- * memory (minus 32), a table side's list is a bitmap there, else a hash
- * table.  bitmap_log2 0 always uses hash tables; otherwise in [10, 17].
- * overlap != 0 runs a hybrid count's HLL pass on a second stream beside the
- * exact pairs (joined before the call returns).  out2 receives the two
- * values.  Results are identical for every setting.  These kernels read
- * col_idx values as vertex indices: a value outside [0, n_nodes) is
- * reported as TCHLL_STATUS_BAD_KEY. */
-int tchll_set_count_core(int32_t bitmap_log2, int32_t overlap);
-int tchll_get_count_core(int32_t* out2 /* host */);
+ * some hub table side's forward list; a probe list member outside the core
+ * cannot match.  A table side's list becomes a bitmap in shared memory:
+ * with packed != 0 and a core of at most 131,070 vertices the probe lists
+ * hold 16-bit core indices (two planes) and the bitmap takes 16 KB; else,
+ * when the core fits 8 * 2^bitmap_log2 bits (minus 32), 32-bit lists and a
+ * bitmap of that size; else hash tables.  bitmap_log2 0 turns the 32-bit
+ * bitmap off; otherwise in [10, 17].  overlap != 0 runs a hybrid count's HLL
+ * pass on a second stream beside the exact pairs (joined before the call
+ * returns).  out3 receives the three values.  Results are identical for
+ * every setting.  These kernels read col_idx values as vertex indices: a
+ * value outside [0, n_nodes) is reported as TCHLL_STATUS_BAD_KEY. */
+int tchll_set_count_core(int32_t bitmap_log2, int32_t overlap, int32_t packed);
+int tchll_get_count_core(int32_t* out3 /* host */);
 
-/* HLL pass of the hybrid counts: for p <= onepass_max_p one pass over both
- * register rows of an edge forms the zero count and the exact sum of 2^-r
- * together; above it the rows' zero masks are read first and the registers
- * only when linear counting cannot apply.  lanes: lanes per HLL edge (0:
- * chosen by p, else a power of two in [1, 32]).  out2 receives both values.
- * Results are identical for every setting. */
-int tchll_set_hll_pass(int32_t onepass_max_p, int32_t lanes);
+/* HLL pass of the hybrid counts (with the zero masks in the workspace):
+ * for p <= row_cache_max_p each group of lanes takes a contiguous run of the
+ * HLL edges (CSR order, so mostly one u) and keeps u's zero mask and
+ * register row in registers, reading only v's per edge.  lanes: lanes per
+ * HLL edge (0: chosen by p, else a power of two in [1, 32]).  out2 receives
+ * both values.  Results are identical for every setting. */
+int tchll_set_hll_pass(int32_t row_cache_max_p, int32_t lanes);
 int tchll_get_hll_pass(int32_t* out2 /* host */);
 
 /*

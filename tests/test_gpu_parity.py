@@ -323,11 +323,14 @@ def test_hub_kernel_settings_match_oracle(tchll, oracle, dev):
 
 
 def test_hub_core_bitmap_hash_and_overlap_match_oracle(tchll, oracle, dev):
-    """The hub kernels in core coordinates: the shared-memory bitmap (core
+    """The hub kernels in core coordinates: packed 16-bit probe lists with a
+    16 KB bitmap, 32-bit lists with a bitmap of the configured size (core
     fits), hash tables only (bitmap off), a bitmap buffer too small for the
     core (the bitmap kernel steps aside on the device and the hash kernel
     counts), each with the hybrid's HLL pass on the side stream or inline:
-    exact counts and hybrid result blocks identical and equal to the oracle."""
+    exact counts and hybrid result blocks identical and equal to the oracle.
+    (Two-plane packed lists, a core above 65,535 vertices, run in the R-MAT
+    scale-22 test.)"""
     import torch
     from triangle_counting_hll_b200 import core
     u, v = core.gen_rmat(16, 16, 0.57, 0.19, 0.19, seed=11, device=dev)
@@ -347,15 +350,16 @@ def test_hub_core_bitmap_hash_and_overlap_match_oracle(tchll, oracle, dev):
     base = core.get_count_tuning()
     blocks = []
     try:
-        for hub, blg, ov in ((128, 15, 1), (128, 0, 1), (64, 10, 0), (64, 15, 0), (128, 12, 1), (200, 17, 1)):
+        for hub, blg, ov, pk in ((128, 15, 1, 1), (128, 15, 1, 0), (128, 0, 1, 0), (64, 10, 0, 0), (64, 15, 0, 1),
+                                 (128, 12, 1, 0), (200, 17, 1, 0), (64, 0, 0, 1)):
             core.set_count_tuning(base["chunk"], base["slots_log2"], base["tiny"], base["blocks_per_sm"], hub=hub,
-                                  bitmap_lg=blg, overlap=bool(ov))
+                                  bitmap_lg=blg, overlap=bool(ov), packed=bool(pk))
             assert core.get_count_tuning()["bitmap_lg"] == blg
-            assert _exact(core, g) == want, (hub, blg, ov)
+            assert _exact(core, g) == want, (hub, blg, ov, pk)
             res, _ = core.hybrid_count_compact_tensors(g.row_ptr, g.col_idx, g.edge_u, g.edge_v, g.degrees, rows,
                                                        slot, p, theta, split_kernels=True)
             tot, r = core.hybrid_from_result(res)
-            assert tot == pytest.approx(otot, rel=HYB_RTOL), (hub, blg, ov)
+            assert tot == pytest.approx(otot, rel=HYB_RTOL), (hub, blg, ov, pk)
             assert (int(r.n_approx), int(r.n_exact), int(r.n_clamped)) == \
                 (ost["n_approx"], ost["n_exact"], ost["n_clamped"])
             blocks.append(bytes(_np(res)))
@@ -580,11 +584,11 @@ def test_hybrid_zero_masks_give_identical_results(tchll, oracle, dev, p):
 
 @pytest.mark.parametrize("p", [4, 8, 10, 12, 16])
 def test_hll_pass_settings_give_identical_results(tchll, oracle, dev, p):
-    """The HLL pass as one pass over both register rows (byte-permute table
-    for ranks <= 7, exact 64-bit sums above) and as zero masks first, at
-    every group width: byte-identical result blocks, equal to the oracle.
-    Includes rows with high ranks (a 5000-clique's hub sketches) so the
-    byte-by-byte branch runs."""
+    """The HLL pass with u's register row cached across a group's run of
+    edges and without it, at several group widths (the byte-permute table
+    for ranks <= 7 and exact 64-bit sums above in both): byte-identical
+    result blocks, equal to the oracle.  Includes rows with high ranks (a
+    2000-clique's sketches) so the byte-by-byte branch runs."""
     import torch
     from triangle_counting_hll_b200 import core
     u, v = core.gen_rmat(14, 16, 0.57, 0.19, 0.19, seed=13, device=dev)
@@ -604,13 +608,13 @@ def test_hll_pass_settings_give_identical_results(tchll, oracle, dev, p):
     base = core.get_count_tuning()
     blocks = []
     try:
-        for onepass_p, lanes in ((10, 0), (16, 0), (0, 0), (16, 1), (16, 4), (16, 32), (0, 2), (0, 32)):
-            core.set_count_tuning(**{**base, "hll_onepass_p": onepass_p, "hll_lanes": lanes})
+        for row_p, lanes in ((10, 0), (16, 0), (0, 0), (16, 2), (16, 4), (16, 32), (0, 2), (0, 32)):
+            core.set_count_tuning(**{**base, "hll_row_cache_p": row_p, "hll_lanes": lanes})
             res, _ = core.hybrid_count_compact_tensors(g.row_ptr, g.col_idx, g.edge_u, g.edge_v, g.degrees, rows,
                                                        slot, p, theta, split_kernels=True)
             tot, r = core.hybrid_from_result(res)
-            assert tot == pytest.approx(otot, rel=HYB_RTOL), (onepass_p, lanes)
-            assert (int(r.n_approx), int(r.n_clamped)) == (ost["n_approx"], ost["n_clamped"]), (onepass_p, lanes)
+            assert tot == pytest.approx(otot, rel=HYB_RTOL), (row_p, lanes)
+            assert (int(r.n_approx), int(r.n_clamped)) == (ost["n_approx"], ost["n_clamped"]), (row_p, lanes)
             blocks.append(bytes(_np(res)))
     finally:
         core.set_count_tuning(**base)

@@ -704,10 +704,11 @@ struct HubParams {
     const int32_t* col_idx;
     int64_t nnz;
     const int32_t* hy;  // y of each hub pair, grouped by x
-    const int32_t* pcol;  // core-filtered padded lists (core_pad_kernel) or null: raw lists
+    const int32_t* pcol;  // padded lists in core coordinates (core_pad_kernel) or null: raw lists
     const int32_t* cidx;  // core index of each vertex, -1 outside the core (with pcol)
-    const int32_t* plen;  // filtered length of each probe list (with pcol)
-    const int32_t* n_core;  // device scalar: core size C (with pcol)
+    const int32_t* n_core;  // device: core size C, vertex of core index kPlane (with pcol)
+    const int2* pl;         // packed lists: {plane-0 units, all units} per row
+    int packed;             // packed 16-bit lists when C <= kCore16Max
     const HubSeg* segs;
     const unsigned long long* n_segs;
     int64_t max_segs;
@@ -724,9 +725,8 @@ struct HubParams {
 // orientation by (degree, id) puts every long list's members among the
 // highest-degree vertices).  The hub kernels work in core coordinates:
 //   * cidx[w] = rank of w among the core vertices (ascending id), else -1;
-//   * each probe list is rewritten as the core indices of its members only
-//     (keys outside the core can never hit, 31% of the hub probes on R-MAT
-//     scale 22), padded with the never-set sentinel C (the core size);
+//   * each probe list is rewritten in core indices, a member outside the
+//     core becoming the sentinel C (the core size), which can never hit;
 //   * a table side's list becomes a C-bit bitmap in shared memory (13.5 KB
 //     on R-MAT scale 22), so a probe is one shift, one 4-byte shared load
 //     and one funnel shift.
@@ -778,53 +778,146 @@ __global__ void core_mark_kernel(const int32_t* __restrict__ row_ptr, int64_t n_
 // After the exclusive scan pos = scan(flag) over n_nodes + 1 entries (flag[n]
 // = 0): cidx[w] = pos[w] for flagged w, else -1 (written over flag), and
 // *n_core = pos[n_nodes].
+// Packed probe lists hold a core index in 16 bits plus a plane: plane 0 the
+// indices below kPlane, plane 1 the others minus kPlane, each plane padded
+// with 0xFFFF.  In the bitmap, core index c sits at bit c (plane 0) or c + 1
+// (plane 1), so bit 65535 (plane 0's padding) and bit 131071 (plane 1's) are
+// never set; that works while C <= kCore16Max.
+constexpr int32_t kPlane = 65535;
+constexpr int32_t kCore16Max = 131070;
+
+// n_core[1] (set to -1 before) receives the vertex of core index kPlane.
 __global__ void core_index_kernel(int32_t* flag_cidx, const int32_t* __restrict__ pos, int64_t n_nodes,
                                   int32_t* n_core) {
     for (int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; w <= n_nodes;
          w += (int64_t)gridDim.x * blockDim.x) {
-        if (w == n_nodes) *n_core = __ldg(pos + n_nodes);
-        else flag_cidx[w] = flag_cidx[w] ? __ldg(pos + w) : -1;
+        if (w == n_nodes) {
+            n_core[0] = __ldg(pos + n_nodes);
+        } else {
+            const bool f = flag_cidx[w] != 0;
+            const int32_t c = __ldg(pos + w);
+            flag_cidx[w] = f ? c : -1;
+            if (f && c == kPlane) n_core[1] = (int32_t)w;
+        }
     }
 }
 
-// Core-filtered padded probe lists, one warp per row: the core indices of
-// N+(y)'s core members in list order, then the sentinel C up to a multiple
-// of 4; plen[y] = number of core members.  Malformed rows get length 0 and a
-// status flag (the counting kernels flag them too when an edge uses them).
-__global__ void core_pad_kernel(const int32_t* __restrict__ row_ptr, int64_t n_nodes, int64_t nnz,
-                                const int32_t* __restrict__ col, const int32_t* __restrict__ cidx,
-                                const int32_t* __restrict__ n_core, int32_t* __restrict__ pcol,
-                                int32_t* __restrict__ plen, tchll_count_result* result) {
-    const int lane = threadIdx.x & 31;
-    const unsigned lt = (1u << lane) - 1u;
-    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    const int32_t C = *n_core;
+// Packed probe lists (used when C <= kCore16Max; core_pad_kernel writes the
+// 32-bit ones otherwise): row y starts at uint16 index pad16_start(y), a
+// multiple of 8 (16 bytes); plane 0 (members below the vertex of core index
+// kPlane) takes lo_units 16-byte units, plane 1 the next ones; pl[y] =
+// {lo_units, all units}.  roundup8(row_ptr[y]) + 24 y leaves room for both
+// planes' padding (at most 7 each) of every row before y.  Rows are sorted
+// (as every CSR of the reference is), so the planes split the row at one
+// position P, found by binary search; a member on the wrong side of P (an
+// unsorted row) or outside the core becomes padding and cannot match.
+__device__ __forceinline__ int64_t pad16_start(int32_t rs, int32_t y) {
+    return (((int64_t)rs + 7) & ~(int64_t)7) + 24 * (int64_t)y;
+}
+
+__device__ __forceinline__ uint32_t plane_key(const int32_t* __restrict__ col, const int32_t* __restrict__ cidx,
+                                              int64_t n_nodes, int32_t i, int plane, uint32_t& status) {
+    const int32_t w = __ldg(col + i);
+    if ((uint64_t)(uint32_t)w >= (uint64_t)n_nodes) {
+        status |= ST_BAD_KEY;
+        return 0xFFFFu;
+    }
+    const int32_t c = __ldg(cidx + w);
+    if (plane == 0) return (c >= 0 && c < kPlane) ? (uint32_t)c : 0xFFFFu;
+    return c >= kPlane ? (uint32_t)(c - kPlane) : 0xFFFFu;
+}
+
+__global__ void core_pad16_kernel(const int32_t* __restrict__ row_ptr, int64_t n_nodes, int64_t nnz,
+                                  const int32_t* __restrict__ col, const int32_t* __restrict__ cidx,
+                                  const int32_t* __restrict__ n_core, int packed, uint16_t* __restrict__ pcol16,
+                                  int2* __restrict__ pl, tchll_count_result* result) {
+    const int32_t C = n_core[0];
+    if (!packed || C > kCore16Max) return;  // grid-uniform: the 32-bit lists apply
+    const int32_t wsplit = n_core[1];       // -1: no plane 1
+    const int sub = threadIdx.x & 7;        // 8 lanes per row, one 16-byte unit each
+    const int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 3;
+    const int64_t ng = ((int64_t)gridDim.x * blockDim.x) >> 3;
     uint32_t status = 0;
-    for (int64_t y = warp; y < n_nodes; y += nwarps) {
+    for (int64_t y = g; y < n_nodes; y += ng) {
         const int32_t rs = __ldg(row_ptr + y), re = __ldg(row_ptr + y + 1);
-        int32_t len = 0;
         if (rs < 0 || re < rs || (int64_t)re > nnz) {
             status |= ST_BAD_ROW;
-        } else {
-            const int64_t ps = pad_start(rs, (int32_t)y);
-            for (int32_t i0 = rs; i0 < re; i0 += 32) {  // warp-uniform
-                int32_t c = -1;
-                if (i0 + lane < re) {
-                    const int32_t w = __ldg(col + i0 + lane);
-                    if ((uint64_t)(uint32_t)w < (uint64_t)n_nodes) c = __ldg(cidx + w);
-                    else status |= ST_BAD_KEY;
-                }
-                const unsigned bal = __ballot_sync(FULL, c >= 0);
-                if (c >= 0) pcol[ps + len + __popc(bal & lt)] = c;
-                len += __popc(bal);
-            }
-            if (lane < ((-len) & 3)) pcol[ps + len + lane] = C;
+            if (sub == 0) pl[y] = make_int2(0, 0);
+            continue;
         }
-        if (lane == 0) plen[y] = len;
+        const int32_t d = re - rs;
+        int32_t P = d;
+        if (wsplit >= 0) {  // first member >= wsplit
+            int32_t lo = 0, hi = d;
+            while (lo < hi) {
+                const int32_t mid = (lo + hi) >> 1;
+                if (__ldg(col + rs + mid) < wsplit) lo = mid + 1; else hi = mid;
+            }
+            P = lo;
+        }
+        const int32_t lo_units = (P + 7) >> 3, units = lo_units + ((d - P + 7) >> 3);
+        const int64_t ps = pad16_start(rs, (int32_t)y);
+        for (int32_t u = sub; u < units; u += 8) {
+            const int plane = u < lo_units ? 0 : 1;
+            const int32_t m0 = plane == 0 ? 8 * u : P + 8 * (u - lo_units);
+            const int32_t end = plane == 0 ? P : d;
+            uint32_t k[8];
+#pragma unroll
+            for (int t = 0; t < 8; ++t)
+                k[t] = (m0 + t < end) ? plane_key(col, cidx, n_nodes, rs + m0 + t, plane, status) : 0xFFFFu;
+            *reinterpret_cast<uint4*>(pcol16 + ps + 8 * u) =
+                make_uint4(k[0] | (k[1] << 16), k[2] | (k[3] << 16), k[4] | (k[5] << 16), k[6] | (k[7] << 16));
+        }
+        if (sub == 0) pl[y] = make_int2(lo_units, units);
     }
     status = __reduce_or_sync(FULL, status);
-    if (lane == 0 && status) atomicOr(&result->status, status);
+    if ((threadIdx.x & 31) == 0 && status) atomicOr(&result->status, status);
+}
+
+// Probe lists in core coordinates, padded: 8 lanes per row, one 16-byte
+// quad each; a member outside the core becomes the sentinel C (a bit that is
+// never set: it cannot match), and so does the padding.  Rows keep their
+// lengths, so a pair's probe list is [pad_start(y), + roundup4(d+(y))).
+// Malformed rows are skipped with a status flag (the counting kernels flag
+// them too when an edge uses them).
+__global__ void core_pad_kernel(const int32_t* __restrict__ row_ptr, int64_t n_nodes, int64_t nnz,
+                                const int32_t* __restrict__ col, const int32_t* __restrict__ cidx,
+                                const int32_t* __restrict__ n_core, int packed, int32_t* __restrict__ pcol,
+                                tchll_count_result* result) {
+    const int32_t C = n_core[0];
+    if (packed && C <= kCore16Max) return;  // grid-uniform: core_pad16_kernel writes the lists
+    const int sub = threadIdx.x & 7;
+    const int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 3;
+    const int64_t ng = ((int64_t)gridDim.x * blockDim.x) >> 3;
+    uint32_t status = 0;
+    for (int64_t y = g; y < n_nodes; y += ng) {
+        const int32_t rs = __ldg(row_ptr + y), re = __ldg(row_ptr + y + 1);
+        if (rs < 0 || re < rs || (int64_t)re > nnz) {
+            status |= ST_BAD_ROW;
+            continue;
+        }
+        const int32_t d = re - rs;
+        const int64_t ps = pad_start(rs, (int32_t)y);  // a multiple of 4: 16-byte aligned stores
+        for (int32_t i = 4 * sub; i < d; i += 32) {
+            int32_t c[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                c[k] = C;
+                if (i + k < d) {
+                    const int32_t w = __ldg(col + rs + i + k);
+                    if ((uint64_t)(uint32_t)w < (uint64_t)n_nodes) {
+                        const int32_t x = __ldg(cidx + w);
+                        c[k] = x >= 0 ? x : C;
+                    } else {
+                        status |= ST_BAD_KEY;
+                    }
+                }
+            }
+            *reinterpret_cast<int4*>(pcol + ps + i) = make_int4(c[0], c[1], c[2], c[3]);
+        }
+    }
+    status = __reduce_or_sync(FULL, status);
+    if ((threadIdx.x & 31) == 0 && status) atomicOr(&result->status, status);
 }
 
 template <int UNR, bool PAD>
@@ -833,7 +926,8 @@ __global__ void __launch_bounds__(256, 5) hub_count_kernel(const HubParams H) {
     __shared__ HubSeg s_seg;
     __shared__ int s_round;
     __shared__ int s_fail;
-    if (PAD && H.cap_bits > 0 && *H.n_core + 32 <= H.cap_bits) return;  // the bitmap kernel counted every segment
+    if (PAD && ((H.packed && *H.n_core <= kCore16Max) || (H.cap_bits > 0 && *H.n_core + 32 <= H.cap_bits)))
+        return;  // a bitmap kernel counted every segment
     const int tid = threadIdx.x, lane = tid & 31;
     const int32_t* __restrict__ col = H.col_idx;
     const int64_t nseg = min((int64_t)*H.n_segs, H.max_segs);
@@ -898,7 +992,7 @@ __global__ void __launch_bounds__(256, 5) hub_count_kernel(const HubParams H) {
                 re = __ldg(H.row_ptr + y + 1);
                 if (PAD) {
                     vs = (int32_t)pad_start(rs, y);
-                    ve = vs + ((__ldg(H.plen + y) + 3) & ~3);
+                    ve = vs + ((re - rs + 3) & ~3);
                 } else {
                     vs = rs;
                     ve = re;
@@ -1054,7 +1148,7 @@ __global__ void __launch_bounds__(256, 5) hub_count_kernel(const HubParams H) {
 // lanes (coalesced loads).  A lane finds its quad's list from the bitmap B
 // of list starts inside its window (one OR-reduction per window): list index
 // = starts before the window + starts up to the lane - 1.  Since the probe
-// lists are core-filtered and padded with the never-set bit C, a key needs no
+// lists are in core coordinates and padded with the never-set bit C, a key needs no
 // mask and no bound: hit = bit key of the bitmap.
 template <int UNR>
 __global__ void __launch_bounds__(256, 6) hub_bitmap_kernel(const HubParams H) {
@@ -1063,7 +1157,7 @@ __global__ void __launch_bounds__(256, 6) hub_bitmap_kernel(const HubParams H) {
     __shared__ int s_round;
     __shared__ int s_fail;
     const int C = *H.n_core;
-    if (C + 32 > H.cap_bits) return;  // grid-uniform: the hash kernel takes over
+    if ((H.packed && C <= kCore16Max) || C + 32 > H.cap_bits) return;  // grid-uniform: another kernel counts
     const int tid = threadIdx.x, lane = tid & 31;
     const unsigned lane_le = (2u << lane) - 1u;  // lane 31: 0 - 1 = all bits
     const uint32_t sentinel = (uint32_t)C;
@@ -1115,12 +1209,9 @@ __global__ void __launch_bounds__(256, 6) hub_bitmap_kernel(const HubParams H) {
             if (lane < np) {
                 const int32_t y = __ldg(H.hy + sg.start + r + lane);
                 rs = __ldg(H.row_ptr + y);
-                if (table) {
-                    vs = (int32_t)pad_start(rs, y);
-                    nq = (__ldg(H.plen + y) + 3) >> 2;
-                } else {
-                    re = __ldg(H.row_ptr + y + 1);
-                }
+                re = __ldg(H.row_ptr + y + 1);
+                vs = (int32_t)pad_start(rs, y);
+                nq = (re - rs + 3) >> 2;
             }
             if (!table) {  // binary search per pair over the raw lists
                 for (int j = 0; j < np; ++j) {
@@ -1177,6 +1268,165 @@ __global__ void __launch_bounds__(256, 6) hub_bitmap_kernel(const HubParams H) {
                 uint32_t c = 0;
 #pragma unroll
                 for (int t = 0; t < 4 * UNR; ++t) c += __funnelshift_r(bm[key[t] >> 5], 0u, key[t]) & 1u;
+                acc += c;
+            }
+        }
+        if (H.batched) {  // this segment's totals belong to its graph
+            acc = warp_sum_u64(acc);
+            if (lane == 0 && acc) atomicAdd((unsigned long long*)&H.result[sg.graph].exact, (unsigned long long)acc);
+            if (tid == 0) atomicAdd((unsigned long long*)&H.result[sg.graph].n_exact, (unsigned long long)sg.len);
+            acc = 0;
+            n_pairs = 0;
+        }
+        __syncthreads();  // every warp is done with this bitmap
+    }
+    if (H.batched) return;
+    acc = warp_sum_u64(acc);
+    n_pairs = warp_sum_i64(n_pairs);
+    if (lane == 0) {
+        if (acc) atomicAdd((unsigned long long*)&H.result->exact, (unsigned long long)acc);
+        if (n_pairs) atomicAdd((unsigned long long*)&H.result->n_exact, (unsigned long long)n_pairs);
+    }
+}
+
+// hub_bitmap_kernel over packed probe lists (C <= kCore16Max): 8 keys per
+// 16-byte unit, so the probe lists, which all pairs read from L2 or HBM, take
+// half the bytes.  The bitmap has 65,536 bits (C <= 65535) or 131,072 bits
+// (16 KB of shared memory); a unit's plane (the bitmap's half) follows from
+// its position in the list: units at or past the list's plane-0 units are
+// plane 1.  Otherwise as hub_bitmap_kernel.
+template <int UNR>
+__global__ void __launch_bounds__(256, 8) hub_bitmap16_kernel(const HubParams H) {
+    extern __shared__ __align__(16) uint32_t bm[];  // 4096 words
+    __shared__ HubSeg s_seg;
+    __shared__ int s_round;
+    __shared__ int s_fail;
+    const int C = H.n_core[0];
+    if (!H.packed || C > kCore16Max) return;  // grid-uniform: a 32-bit kernel counts
+    const int tid = threadIdx.x, lane = tid & 31;
+    const unsigned lane_le = (2u << lane) - 1u;
+    const int nw4 = C > kPlane ? 1024 : 512;  // uint4 words: 131,072 or 65,536 bits
+    const int32_t* __restrict__ col = H.col_idx;
+    const uint4* __restrict__ pq = reinterpret_cast<const uint4*>(H.pcol);
+    const int64_t nseg = min((int64_t)*H.n_segs, H.max_segs);
+    uint64_t acc = 0;
+    int64_t n_pairs = 0;
+    while (true) {
+        if (tid == 0) {
+            const unsigned long long s = atomicAdd(H.seg_ctr, 1ull);
+            if ((int64_t)s < nseg) {
+                s_seg = H.segs[s];
+            } else {
+                s_seg.x = -1;
+                s_seg.len = 0;
+                s_seg.start = 0;
+            }
+            s_round = 0;
+            s_fail = 0;
+        }
+        for (int i = tid; i < nw4; i += blockDim.x) reinterpret_cast<uint4*>(bm)[i] = make_uint4(0u, 0u, 0u, 0u);
+        __syncthreads();
+        const HubSeg sg = s_seg;
+        if (sg.x < 0) break;
+        if (tid == 0) n_pairs += sg.len;
+        const int32_t xs = __ldg(H.row_ptr + sg.x);
+        const int xl = __ldg(H.row_ptr + sg.x + 1) - xs;
+        for (int i = tid; i < xl; i += blockDim.x) {
+            const int32_t w = __ldg(col + xs + i);
+            const int32_t c = (uint64_t)(uint32_t)w < (uint64_t)H.n_nodes ? __ldg(H.cidx + w) : -1;
+            if (c >= 0) {
+                const int32_t bit = c < kPlane ? c : c + 1;
+                atomicOr(bm + (bit >> 5), 1u << (bit & 31));
+            } else {
+                s_fail = 1;  // not in the core (cannot happen for well-formed input)
+            }
+        }
+        __syncthreads();
+        const bool table = !s_fail;  // CTA-uniform
+        int rsz = (sg.len + 15) >> 4;
+        rsz = rsz < 4 ? 4 : (rsz > 32 ? 32 : rsz);
+        while (true) {
+            int r = 0;
+            if (lane == 0) r = atomicAdd(&s_round, rsz);
+            r = __shfl_sync(FULL, r, 0);
+            if (r >= sg.len) break;
+            const int np = min(rsz, sg.len - r);
+            int32_t q0 = 0, nq = 0, lo = 0, rs = 0, re = 0;
+            if (lane < np) {
+                const int32_t y = __ldg(H.hy + sg.start + r + lane);
+                rs = __ldg(H.row_ptr + y);
+                re = __ldg(H.row_ptr + y + 1);
+                const int2 u = H.pl[y];
+                q0 = (int32_t)(pad16_start(rs, y) >> 3);
+                lo = u.x;
+                nq = u.y;
+            }
+            if (!table) {  // binary search per pair over the raw lists
+                for (int j = 0; j < np; ++j) {
+                    const int32_t jrs = __shfl_sync(FULL, rs, j);
+                    const int32_t jre = __shfl_sync(FULL, re, j);
+                    acc += warp_bsearch_count(col + xs, xl, col + jrs, jre - jrs, lane);
+                }
+                continue;
+            }
+            const unsigned ne = __ballot_sync(FULL, nq > 0);
+            const int k = __popc(ne);
+            const int src = lane < k ? (int)__fns(ne, 0, lane + 1) : lane;
+            const int c_q0 = __shfl_sync(FULL, q0, src);
+            int c_nq = __shfl_sync(FULL, nq, src);
+            const int c_lo = __shfl_sync(FULL, lo, src);
+            if (lane >= k) c_nq = 0;
+            int incl = c_nq;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += t;
+            }
+            const int excl = incl - c_nq;
+            const int W = __shfl_sync(FULL, incl, 31);
+            const int qb = c_q0 - excl;   // unit of stream position t in list j: qb[j] + t
+            const int thr = excl + c_lo;  // stream positions >= thr[j] are list j's plane 1
+            const bool starts = lane < k;
+            int S = 0;
+            for (int T0 = 0; T0 < W; T0 += 32 * UNR) {
+                int qd[UNR], hw[UNR];
+#pragma unroll
+                for (int i = 0; i < UNR; ++i) {
+                    const int Ti = T0 + 32 * i;
+                    qd[i] = -1;
+                    hw[i] = 0;
+                    if (Ti < W) {  // warp-uniform
+                        const unsigned d = (unsigned)(excl - Ti);
+                        const unsigned B = __reduce_or_sync(FULL, (starts && d < 32u) ? (1u << d) : 0u);
+                        const int j = (S + __popc(B & lane_le) - 1) & 31;
+                        S += __popc(B);
+                        const int my_qb = __shfl_sync(FULL, qb, j);
+                        const int my_thr = __shfl_sync(FULL, thr, j);
+                        const int t = Ti + lane;
+                        if (t < W) {
+                            qd[i] = my_qb + t;
+                            hw[i] = t >= my_thr ? 2048 : 0;  // plane 1: the bitmap's upper half
+                        }
+                    }
+                }
+                uint4 q[UNR];
+#pragma unroll
+                for (int i = 0; i < UNR; ++i) {
+                    q[i] = make_uint4(~0u, ~0u, ~0u, ~0u);  // padding keys: bit 65535, never set
+                    if (qd[i] >= 0) q[i] = __ldg(pq + qd[i]);
+                }
+                uint32_t c = 0;
+#pragma unroll
+                for (int i = 0; i < UNR; ++i) {
+                    const uint32_t* b = bm + hw[i];
+                    const uint32_t w4[4] = {q[i].x, q[i].y, q[i].z, q[i].w};
+#pragma unroll
+                    for (int t = 0; t < 4; ++t) {
+                        const uint32_t w = w4[t];
+                        c += __funnelshift_r(b[(w >> 5) & 0x7FFu], 0u, w) & 1u;
+                        c += __funnelshift_r(b[w >> 21], 0u, w >> 16) & 1u;
+                    }
+                }
                 acc += c;
             }
         }
@@ -1395,23 +1645,22 @@ __device__ __forceinline__ double hll_estimate_from(U128 zsum, double extra, uin
 }
 
 // One group of L lanes per HLL edge, the group's lanes striding over the two
-// 2^p-byte rows with 16-byte loads.
-//   ONEPASS (p <= 10, where most edges need every register): one pass over
-//     both rows forms the zero count and the exact sum together.
-//   otherwise: pass 1 counts the zero registers V of the merged row from the
-//     AND of the two rows' zero masks (ZM; else from the registers).  Every
-//     zero register adds exactly 1 to Z = sum 2^-r, so V >= lc_min (the
-//     smallest V with alpha*m^2/V <= 2.5m, with a 1e-9 margin for the FP64
-//     comparison) proves the estimator takes its linear-counting branch: E =
-//     m * ln(m / V), the same expression the full estimator evaluates, and Z
-//     is not needed.  Otherwise pass 2 forms Z exactly and applies the full
-//     estimator.
+// 2^p-byte rows with 16-byte loads.  Pass 1 counts the zero registers V of
+// the merged row from the AND of the two rows' zero masks (ZM; else from the
+// registers).  Every zero register adds exactly 1 to Z = sum 2^-r, so V >=
+// lc_min (the smallest V with alpha*m^2/V <= 2.5m, with a 1e-9 margin for
+// the FP64 comparison) proves the estimator takes its linear-counting
+// branch: E = m * ln(m / V), the same expression the full estimator
+// evaluates, and Z is not needed.  Otherwise pass 2 forms Z exactly and
+// applies the full estimator.
 // CACHE: each group takes a contiguous run of the edge list.  The routing
-// pass appends edges in CSR order, so consecutive HLL edges mostly share u
+// pass appends edges in CSR order, so consecutive HLL edges mostly share u,
 // and the group keeps u's zero mask in registers across them (up to four
-// 16-byte words per lane).  Otherwise the groups stride over the list.
-template <int L, bool ZM, bool CACHE, bool ONEPASS>
-__global__ void __launch_bounds__(256, CACHE ? 3 : 4) hll_edges_kernel(const HllParams H) {
+// 16-byte words per lane) and, with CROW (rows of at most 8 16-byte words
+// per lane), u's register row too: an edge then reads only v's mask and
+// row.  Otherwise the groups stride over the list.
+template <int L, bool ZM, bool CACHE, bool CROW>
+__global__ void __launch_bounds__(256, CROW ? 2 : (CACHE ? 3 : 4)) hll_edges_kernel(const HllParams H) {
     const int lane = threadIdx.x & 31;
     const int sub = lane & (L - 1);
     const unsigned gmask = (L == 32) ? FULL : (((1u << L) - 1u) << (lane & ~(L - 1)));
@@ -1428,9 +1677,11 @@ __global__ void __launch_bounds__(256, CACHE ? 3 : 4) hll_edges_kernel(const Hll
     const int64_t e_hi = CACHE ? min(n, e_lo + per) : n;
     const int64_t e_step = CACHE ? 1 : ngroups;
     const int nq = H.zst >> 2;
-    const bool cache_a = CACHE && ZM && nq <= 4 * L;
-    int64_t cached = -1;
-    uint4 ca[4];
+    constexpr int KA = CROW ? 1 : 4;  // mask words cached per lane (p <= 10 with a cached row: one)
+    const bool cache_a = CACHE && ZM && nq <= KA * L;
+    int64_t cached = -1, cached_row = -1;
+    uint4 ca[KA];
+    uint4 ra[CROW ? 8 : 1];
     for (int64_t e = e_lo; e < e_hi; e += e_step) {
         const int32_t u = __ldg(H.hu + e), v = __ldg(H.hv + e);
         const int64_t su = H.slot ? __ldg(H.slot + u) : (int64_t)u;
@@ -1438,73 +1689,70 @@ __global__ void __launch_bounds__(256, CACHE ? 3 : 4) hll_edges_kernel(const Hll
         const uint4* a4 = reinterpret_cast<const uint4*>(H.regs + su * (int64_t)m);
         const uint4* b4 = reinterpret_cast<const uint4*>(H.regs + sv * (int64_t)m);
         double E;
-        if (ONEPASS) {
-            uint32_t fast = 0, zeros = 0;
-            uint64_t fine = 0;
-            double extra = 0.0;
+        uint32_t zeros = 0;
+        if (ZM) {  // registers zero in both rows: AND of the two zero masks
+            const uint4* za = reinterpret_cast<const uint4*>(H.zm + su * (int64_t)H.zst);
+            const uint4* zb = reinterpret_cast<const uint4*>(H.zm + sv * (int64_t)H.zst);
+            if (cache_a) {
+                if (su != cached) {  // group-uniform
+#pragma unroll
+                    for (int k = 0; k < KA; ++k) {
+                        const int i = sub + k * L;
+                        ca[k] = i < nq ? __ldg(za + i) : make_uint4(0u, 0u, 0u, 0u);
+                    }
+                    cached = su;
+                }
+#pragma unroll
+                for (int k = 0; k < KA; ++k) {
+                    const int i = sub + k * L;
+                    if (i < nq) {
+                        const uint4 b = __ldg(zb + i);
+                        zeros += __popc(ca[k].x & b.x) + __popc(ca[k].y & b.y) + __popc(ca[k].z & b.z) +
+                                 __popc(ca[k].w & b.w);
+                    }
+                }
+            } else {
+#pragma unroll 4
+                for (int i = sub; i < nq; i += L) {
+                    const uint4 a = __ldg(za + i), b = __ldg(zb + i);
+                    zeros += __popc(a.x & b.x) + __popc(a.y & b.y) + __popc(a.z & b.z) + __popc(a.w & b.w);
+                }
+            }
+        } else {
 #pragma unroll 4
             for (int i = sub; i < nvec; i += L) {
                 const uint4 a = __ldg(a4 + i), b = __ldg(b4 + i);
-                hll_word_lut(__vmaxu4(a.x, b.x), S, fast, fine, zeros, extra);
-                hll_word_lut(__vmaxu4(a.y, b.y), S, fast, fine, zeros, extra);
-                hll_word_lut(__vmaxu4(a.z, b.z), S, fast, fine, zeros, extra);
-                hll_word_lut(__vmaxu4(a.w, b.w), S, fast, fine, zeros, extra);
+                zeros += zero_bytes(a.x | b.x) + zero_bytes(a.y | b.y) + zero_bytes(a.z | b.z) + zero_bytes(a.w | b.w);
             }
-            fast = group_sum_u32<L>(fast, gmask);
-            zeros = group_sum_u32<L>(zeros, gmask);
-            fine = group_sum_u64<L>(fine, gmask);
-#pragma unroll
-            for (int o = L / 2; o > 0; o >>= 1) extra += __shfl_xor_sync(gmask, extra, o);
-            U128 z;  // fast * 2^(S-7) + fine; fast <= 2^(p+7)
-            z.lo = (uint64_t)fast << (S - 7);
-            z.hi = (uint64_t)fast >> (71 - S);
-            z.add(fine);
-            E = hll_estimate_from(z, extra, zeros, H.p, S, H.variant);
+        }
+        zeros = group_sum_u32<L>(zeros, gmask);
+        if (zeros >= H.lc_min) {
+            E = (double)m * log((double)m / (double)zeros);
         } else {
-            uint32_t zeros = 0;
-            if (ZM) {  // registers zero in both rows: AND of the two zero masks
-                const uint4* za = reinterpret_cast<const uint4*>(H.zm + su * (int64_t)H.zst);
-                const uint4* zb = reinterpret_cast<const uint4*>(H.zm + sv * (int64_t)H.zst);
-                if (cache_a) {
-                    if (su != cached) {  // group-uniform
+            uint32_t fast = 0, zz = 0;
+            uint64_t fine = 0;
+            double extra = 0.0;
+            if (CROW) {
+                if (su != cached_row) {  // group-uniform
 #pragma unroll
-                        for (int k = 0; k < 4; ++k) {
-                            const int i = sub + k * L;
-                            ca[k] = i < nq ? __ldg(za + i) : make_uint4(0u, 0u, 0u, 0u);
-                        }
-                        cached = su;
-                    }
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
+                    for (int k = 0; k < 8; ++k) {
                         const int i = sub + k * L;
-                        if (i < nq) {
-                            const uint4 b = __ldg(zb + i);
-                            zeros += __popc(ca[k].x & b.x) + __popc(ca[k].y & b.y) + __popc(ca[k].z & b.z) +
-                                     __popc(ca[k].w & b.w);
-                        }
+                        ra[k] = i < nvec ? __ldg(a4 + i) : make_uint4(0u, 0u, 0u, 0u);
                     }
-                } else {
-#pragma unroll 4
-                    for (int i = sub; i < nq; i += L) {
-                        const uint4 a = __ldg(za + i), b = __ldg(zb + i);
-                        zeros += __popc(a.x & b.x) + __popc(a.y & b.y) + __popc(a.z & b.z) + __popc(a.w & b.w);
+                    cached_row = su;
+                }
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const int i = sub + k * L;
+                    if (i < nvec) {
+                        const uint4 b = __ldg(b4 + i);
+                        hll_word_lut(__vmaxu4(ra[k].x, b.x), S, fast, fine, zz, extra);
+                        hll_word_lut(__vmaxu4(ra[k].y, b.y), S, fast, fine, zz, extra);
+                        hll_word_lut(__vmaxu4(ra[k].z, b.z), S, fast, fine, zz, extra);
+                        hll_word_lut(__vmaxu4(ra[k].w, b.w), S, fast, fine, zz, extra);
                     }
                 }
             } else {
-#pragma unroll 4
-                for (int i = sub; i < nvec; i += L) {
-                    const uint4 a = __ldg(a4 + i), b = __ldg(b4 + i);
-                    zeros += zero_bytes(a.x | b.x) + zero_bytes(a.y | b.y) + zero_bytes(a.z | b.z) +
-                             zero_bytes(a.w | b.w);
-                }
-            }
-            zeros = group_sum_u32<L>(zeros, gmask);
-            if (zeros >= H.lc_min) {
-                E = (double)m * log((double)m / (double)zeros);
-            } else {
-                uint32_t fast = 0, zz = 0;
-                uint64_t fine = 0;
-                double extra = 0.0;
 #pragma unroll 2
                 for (int i = sub; i < nvec; i += L) {
                     const uint4 a = __ldg(a4 + i), b = __ldg(b4 + i);
@@ -1513,16 +1761,16 @@ __global__ void __launch_bounds__(256, CACHE ? 3 : 4) hll_edges_kernel(const Hll
                     hll_word_lut(__vmaxu4(a.z, b.z), S, fast, fine, zz, extra);
                     hll_word_lut(__vmaxu4(a.w, b.w), S, fast, fine, zz, extra);
                 }
-                fast = group_sum_u32<L>(fast, gmask);
-                fine = group_sum_u64<L>(fine, gmask);
-#pragma unroll
-                for (int o = L / 2; o > 0; o >>= 1) extra += __shfl_xor_sync(gmask, extra, o);
-                U128 z;
-                z.lo = (uint64_t)fast << (S - 7);
-                z.hi = (uint64_t)fast >> (71 - S);
-                z.add(fine);
-                E = hll_estimate_from(z, extra, zeros, H.p, S, H.variant);
             }
+            fast = group_sum_u32<L>(fast, gmask);
+            fine = group_sum_u64<L>(fine, gmask);
+#pragma unroll
+            for (int o = L / 2; o > 0; o >>= 1) extra += __shfl_xor_sync(gmask, extra, o);
+            U128 z;  // fast * 2^(S-7) + fine; fast <= 2^(p+7)
+            z.lo = (uint64_t)fast << (S - 7);
+            z.hi = (uint64_t)fast >> (71 - S);
+            z.add(fine);
+            E = hll_estimate_from(z, extra, zeros, H.p, S, H.variant);
         }
         if (sub == 0) {
             const int32_t du = __ldg(H.degrees + u), dv = __ldg(H.degrees + v);
@@ -1565,7 +1813,8 @@ struct Tuning {
     int hub_unroll = 2;     // quads per lane in flight (2 or 4)
     int bitmap_lg = 15;     // hub bitmap buffer: 2^15 bytes = 262,144 core vertices (0: hash tables only)
     int overlap = 1;        // hybrid: HLL pass on a side stream beside the exact pairs
-    int hll_onepass_p = 10; // HLL pass: one pass over both register rows for p <= this
+    int packed = 1;         // hub probe lists as 16-bit core indices when the core allows
+    int hll_row_cache_p = 10;  // HLL pass: keep u's register row in registers for p <= this
     int hll_lanes = 0;      // HLL pass: lanes per edge (0: chosen by p)
 };
 constexpr int HUB_MIN = 64;       // smallest hub threshold (bounds the segment count)
@@ -1680,19 +1929,25 @@ struct CountWs {
     int32_t* py;              // n_edges (small pairs, then the hub list)
     HubSeg* segs;             // max_segs
     int64_t max_segs;
-    int32_t* pcol;            // core-filtered padded lists for the hub kernels, pcap entries (null: not carved)
+    int32_t* pcol;            // padded lists in core coordinates for the hub kernels, pcap entries (null: not carved)
     int64_t pcap;
     int32_t* cflag;           // n_nodes + 1: core flags, then core indices (with pcol)
     int32_t* cpos;            // n_nodes + 1: scan of the flags (with pcol)
-    int32_t* plen;            // n_nodes: filtered probe-list lengths (with pcol)
-    int32_t* ncore;           // 1: core size (with pcol)
+    int32_t* ncore;           // core size, vertex of core index kPlane (with pcol)
+    int2* pl;                 // n_nodes: packed lists' {plane-0 units, all units} (with pcol)
     void* tmp;
     size_t tmp_bytes;
 };
 
 // Padded lists need nnz + 8 (n_nodes + 1) entries; the workspace holds them
 // for nnz <= n_edges (every oriented edge listed once).
-static int64_t pad_capacity(int64_t n_nodes, int64_t nnz) { return nnz + 8 * (n_nodes + 1) + 8; }
+// int32 entries of the padded-list region: the 32-bit lists (pad_start)
+// or the packed ones (pad16_start, 2 bytes a key), whichever is larger.
+static int64_t pad_capacity(int64_t n_nodes, int64_t nnz) {
+    const int64_t w32 = nnz + 8 * (n_nodes + 1) + 8;
+    const int64_t w16 = (nnz + 24 * (n_nodes + 1) + 24 + 1) / 2 + 4;
+    return w32 > w16 ? w32 : w16;
+}
 
 static bool carve_count(void* ws, size_t bytes, int64_t n_nodes, int64_t n_edges, CountWs& W, size_t* need,
                         bool pad = true) {
@@ -1715,8 +1970,8 @@ static bool carve_count(void* ws, size_t bytes, int64_t n_nodes, int64_t n_edges
     W.pcol = pad ? cv.take<int32_t>((size_t)W.pcap) : nullptr;
     W.cflag = pad ? cv.take<int32_t>(N) : nullptr;
     W.cpos = pad ? cv.take<int32_t>(N) : nullptr;
-    W.plen = pad ? cv.take<int32_t>(N) : nullptr;
     W.ncore = pad ? cv.take<int32_t>(4) : nullptr;
+    W.pl = pad ? cv.take<int2>(N) : nullptr;
     W.tmp_bytes = tb;
     W.tmp = cv.take<char>(tb);
     if (need) *need = cv.off;
@@ -1772,9 +2027,9 @@ static uint32_t lc_min_for(int p) {
 }
 
 template <int L>
-static int launch_hll_edges_L(const HllParams& H, bool onepass, cudaStream_t st) {
+static int launch_hll_edges_L(const HllParams& H, bool crow, cudaStream_t st) {
     const int grid = sm_count() * 8;
-    if (onepass) hll_edges_kernel<L, false, false, true><<<grid, 256, 0, st>>>(H);
+    if (H.zm && crow && L * 8 >= ((1 << H.p) >> 4)) hll_edges_kernel<L, true, true, true><<<grid, 256, 0, st>>>(H);
     else if (H.zm && H.p >= 11) hll_edges_kernel<L, true, true, false><<<grid, 256, 0, st>>>(H);
     else if (H.zm) hll_edges_kernel<L, true, false, false><<<grid, 256, 0, st>>>(H);
     else hll_edges_kernel<L, false, false, false><<<grid, 256, 0, st>>>(H);
@@ -1796,21 +2051,20 @@ static int launch_hll_edges(const CountParams& P, const HybridWs& HW, const Tuni
     H.variant = P.variant;
     H.lc_min = lc_min_for(P.p);
     H.result = P.result;
-    // p <= onepass_p: one pass over both register rows (most edges need
-    // them all; no zero masks).  Otherwise the zero masks first (when the
-    // workspace holds them).
-    const bool onepass = P.p <= T.hll_onepass_p;
-    H.zm = onepass ? nullptr : HW.zm;
-    H.zst = onepass ? 0 : HW.zst;
-    // Group width (lanes per edge, at most a warp).  One pass: m / 128 lanes
-    // (p = 10: 8 lanes of 128 registers each).  With zero masks, for p >= 11
-    // the linear-counting shortcut settles almost every edge from the masks
+    H.zm = HW.zm;
+    H.zst = HW.zst;
+    // p <= row_cache_p (with zero masks): contiguous runs per group with u's
+    // register row kept in registers, m / 128 lanes per edge (8 16-byte
+    // words of the row per lane).  Otherwise: for p >= 11 the
+    // linear-counting shortcut settles almost every edge from the masks
     // alone, a pass bound by the latency of its dependent loads: four mask
-    // loads per lane per row, several edges per warp in flight.  Otherwise
+    // loads per lane per row, several edges per warp in flight; for p = 9, 10
+    // one mask load per lane; for p <= 8 one lane per edge; without masks
     // one 16-byte register load per lane per row.  (Measured on R-MAT scale
     // 22, theta = 256.)  T.hll_lanes > 0 overrides the width.
+    const bool crow = H.zm != nullptr && P.p <= T.hll_row_cache_p;
     int width = (1 << P.p) >> 4;
-    if (onepass) width = (1 << P.p) >> 7;
+    if (crow) width = (1 << P.p) >> 7;
     else if (H.zm) width = P.p >= 11 ? H.zst >> 4 : (P.p >= 9 ? H.zst >> 2 : 1);
     if (T.hll_lanes > 0) width = T.hll_lanes;
     if (H.zm) {
@@ -1821,12 +2075,12 @@ static int launch_hll_edges(const CountParams& P, const HybridWs& HW, const Tuni
         TCHLL_CHECK_LAUNCH("zmask_kernel");
     }
     switch (width >= 32 ? 32 : (width < 1 ? 1 : width)) {
-        case 1: return launch_hll_edges_L<1>(H, onepass, st);
-        case 2: return launch_hll_edges_L<2>(H, onepass, st);
-        case 4: return launch_hll_edges_L<4>(H, onepass, st);
-        case 8: return launch_hll_edges_L<8>(H, onepass, st);
-        case 16: return launch_hll_edges_L<16>(H, onepass, st);
-        default: return launch_hll_edges_L<32>(H, onepass, st);
+        case 1: return launch_hll_edges_L<1>(H, crow, st);
+        case 2: return launch_hll_edges_L<2>(H, crow, st);
+        case 4: return launch_hll_edges_L<4>(H, crow, st);
+        case 8: return launch_hll_edges_L<8>(H, crow, st);
+        case 16: return launch_hll_edges_L<16>(H, crow, st);
+        default: return launch_hll_edges_L<32>(H, crow, st);
     }
 }
 
@@ -1907,7 +2161,7 @@ static int launch_hub(const CountParams& P, const CountWs& W, const Tuning& T, c
     H.seg_ctr = W.ctr + 3;
     H.hub_lg = T.hub_lg;
     H.result = P.result;
-    // core-filtered padded lists when the workspace holds them and quad
+    // padded lists in core coordinates when the workspace holds them and quad
     // indices fit int
     const int64_t need_pad = pad_capacity(P.n_nodes, P.nnz);
     const bool pad = W.pcol != nullptr && need_pad <= W.pcap && need_pad <= (int64_t)INT32_MAX;
@@ -1921,17 +2175,40 @@ static int launch_hub(const CountParams& P, const CountWs& W, const Tuning& T, c
         size_t tb = W.tmp_bytes;
         TCHLL_CUDA(cub::DeviceScan::ExclusiveSum(W.tmp, tb, W.cflag, W.cpos, (int)N, st));
         count_launch();
+        TCHLL_CUDA(cudaMemsetAsync(W.ncore + 1, 0xFF, sizeof(int32_t), st));
         core_index_kernel<<<grid_rows(N, 256), 256, 0, st>>>(W.cflag, W.cpos, P.n_nodes, W.ncore);
         TCHLL_CHECK_LAUNCH("core_index_kernel");
-        core_pad_kernel<<<grid_rows(P.n_nodes, 8), 256, 0, st>>>(P.row_ptr, P.n_nodes, P.nnz, P.col_idx, W.cflag,
-                                                                 W.ncore, W.pcol, W.plen, P.result);
+        // packed 16-bit lists when the core allows it, else 32-bit lists
+        // (each kernel checks the core size on the device)
+        core_pad16_kernel<<<grid_rows(P.n_nodes, 32), 256, 0, st>>>(P.row_ptr, P.n_nodes, P.nnz, P.col_idx,
+                                                                    W.cflag, W.ncore, T.packed,
+                                                                    reinterpret_cast<uint16_t*>(W.pcol), W.pl,
+                                                                    P.result);
+        TCHLL_CHECK_LAUNCH("core_pad16_kernel");
+        core_pad_kernel<<<grid_rows(P.n_nodes, 32), 256, 0, st>>>(P.row_ptr, P.n_nodes, P.nnz, P.col_idx, W.cflag,
+                                                                  W.ncore, T.packed, W.pcol, P.result);
         TCHLL_CHECK_LAUNCH("core_pad_kernel");
         H.pcol = W.pcol;
         H.cidx = W.cflag;
-        H.plen = W.plen;
         H.n_core = W.ncore;
+        H.pl = W.pl;
+        H.packed = T.packed;
     }
     if (ps.active()) cudaEventRecord(g_phase.hub_ev[1], st);
+    if (pad && T.packed) {
+        const size_t smem = 16384;
+        auto kern = T.hub_unroll == 4 ? hub_bitmap16_kernel<4> : hub_bitmap16_kernel<2>;
+        static size_t smem_set[2][kMaxDevices] = {};
+        int rc = ensure_smem((const void*)kern, smem, smem_set[T.hub_unroll == 4 ? 1 : 0],
+                             "cudaFuncSetAttribute(hub_bitmap16_kernel)", true);
+        if (rc) return rc;
+        int bps = 0;
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, 256, smem);
+        if (e != cudaSuccess) return cuda_status(e, "occupancy(hub_bitmap16_kernel)");
+        if (bps < 1) bps = 1;
+        kern<<<sm_count() * bps, 256, smem, st>>>(H);
+        TCHLL_CHECK_LAUNCH("hub_bitmap16_kernel");
+    }
     if (pad && T.bitmap_lg > 0) {
         const size_t smem = (size_t)1 << T.bitmap_lg;
         H.cap_bits = (int)(8 * smem);
@@ -2048,7 +2325,7 @@ static int run_count(CountParams P, int mode, bool details, void* ws, size_t ws_
     size_t need = 0;
     bool ok;
     // Optional parts, used when the workspace has room (same results): the
-    // core-filtered lists of the hub kernels and, for hybrid calls, the zero
+    // core-coordinate lists of the hub kernels and, for hybrid calls, the zero
     // masks that let the HLL pass test linear counting without the registers.
     if (mode == MODE_EXACT) {
         ok = carve_count(ws, ws_bytes, P.n_nodes, P.n_edges, W, &need, true);
@@ -2338,29 +2615,31 @@ TCHLL_EXPORT int tchll_get_count_hub(int32_t* out4) {
     return TCHLL_OK;
 }
 
-TCHLL_EXPORT int tchll_set_count_core(int32_t bitmap_log2, int32_t overlap) {
+TCHLL_EXPORT int tchll_set_count_core(int32_t bitmap_log2, int32_t overlap, int32_t packed) {
     std::lock_guard<std::mutex> lock(g_tuning_mu);
     TCHLL_ARG(bitmap_log2 == 0 || (bitmap_log2 >= 10 && bitmap_log2 <= 17),
               "bitmap_log2 must be 0 (hash tables only) or in [10, 17] (1 KB .. 128 KB of shared memory)");
     g_tuning.bitmap_lg = bitmap_log2;
     g_tuning.overlap = overlap ? 1 : 0;
+    g_tuning.packed = packed ? 1 : 0;
     return TCHLL_OK;
 }
 
-TCHLL_EXPORT int tchll_get_count_core(int32_t* out2) {
-    TCHLL_ARG(out2 != nullptr, "null output");
+TCHLL_EXPORT int tchll_get_count_core(int32_t* out3) {
+    TCHLL_ARG(out3 != nullptr, "null output");
     const Tuning T = tuning_snapshot();
-    out2[0] = T.bitmap_lg;
-    out2[1] = T.overlap;
+    out3[0] = T.bitmap_lg;
+    out3[1] = T.overlap;
+    out3[2] = T.packed;
     return TCHLL_OK;
 }
 
-TCHLL_EXPORT int tchll_set_hll_pass(int32_t onepass_max_p, int32_t lanes) {
+TCHLL_EXPORT int tchll_set_hll_pass(int32_t row_cache_max_p, int32_t lanes) {
     std::lock_guard<std::mutex> lock(g_tuning_mu);
-    TCHLL_ARG(onepass_max_p >= 0 && onepass_max_p <= 16, "onepass_max_p must be in [0, 16]");
+    TCHLL_ARG(row_cache_max_p >= 0 && row_cache_max_p <= 16, "row_cache_max_p must be in [0, 16]");
     TCHLL_ARG(lanes == 0 || (lanes >= 1 && lanes <= 32 && (lanes & (lanes - 1)) == 0),
               "lanes must be 0 (automatic) or a power of two in [1, 32]");
-    g_tuning.hll_onepass_p = onepass_max_p;
+    g_tuning.hll_row_cache_p = row_cache_max_p;
     g_tuning.hll_lanes = lanes;
     return TCHLL_OK;
 }
@@ -2368,7 +2647,7 @@ TCHLL_EXPORT int tchll_set_hll_pass(int32_t onepass_max_p, int32_t lanes) {
 TCHLL_EXPORT int tchll_get_hll_pass(int32_t* out2) {
     TCHLL_ARG(out2 != nullptr, "null output");
     const Tuning T = tuning_snapshot();
-    out2[0] = T.hll_onepass_p;
+    out2[0] = T.hll_row_cache_p;
     out2[1] = T.hll_lanes;
     return TCHLL_OK;
 }

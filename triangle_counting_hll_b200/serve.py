@@ -258,6 +258,7 @@ class Server:
             if r.key in self.building:  # its graph is being built: answer it with that build
                 queue_.popleft()
                 self.building[r.key].append(r)
+                self.stats["cache_hits"] += 1  # one build serves both queries
                 taken += 1
                 continue
             res = self.resident.get(r.key)
