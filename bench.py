@@ -192,6 +192,19 @@ def hub_work(g, hub_thr: int) -> dict:
             "model_bytes": 16 * fquads + 12 * n_pairs + 8 * tables}
 
 
+CORE16_MAX = 131070  # largest core of the packed (16-bit) hub probe lists
+
+
+def hub_kernel_name(tuning: dict, core_vertices: int) -> str:
+    """The hub kernel that counts with this tuning and core size (the library
+    picks it on the device from the same core size)."""
+    if tuning.get("packed") and core_vertices <= CORE16_MAX:
+        return "hub_bitmap16_kernel"
+    if tuning.get("bitmap_lg") and core_vertices + 32 <= 8 << tuning["bitmap_lg"]:
+        return "hub_bitmap_kernel"
+    return "hub_count_kernel"
+
+
 def time_csr_build(dev, scale: int, reps: int = 3) -> dict:
     """The device CSR build (raw R-MAT endpoints in HBM -> dedup, compaction,
     orientation, sorted rows), timed with CUDA events; the reference's
@@ -357,7 +370,7 @@ def run_ours(args):
     del host
 
     peaks = load_peaks()
-    kname = "hub_bitmap_kernel" if hub_avg else "count_kernel<exact>"
+    kname = hub_kernel_name(tuning, hw["core_vertices"]) if hub_avg else "count_kernel<exact>"
     kms = hub_avg if hub_avg else kernel_avg
     traffic = load_traffic(f"{WORKLOAD}:{kname}") if args.scale == SCALE else None
     roof = {"bound": "hbm", "kernel": kname, "unit": "GB/s", "peak": peaks["hbm_gbs"],
@@ -527,7 +540,9 @@ def run_hybrid_line(args, g, dev, rank, world, barrier, max_over_ranks):
     # the others), hub pairs, other exact pairs
     hub_ms = avg.get("hub") or 0.0
     core_ms = avg.get("hub_core") or 0.0
-    cands = [("hll_edges_kernel", avg["hll"], hll_bytes), ("hub_bitmap_kernel", hub_ms, hub_bytes),
+    tuning = core.get_count_tuning()
+    hname = hub_kernel_name(tuning, hub_work(g, tuning["hub"])["core_vertices"])
+    cands = [("hll_edges_kernel", avg["hll"], hll_bytes), (hname, hub_ms, hub_bytes),
              ("count_kernel", avg["count"] - hub_ms - core_ms, exact_bytes - hub_bytes)]
     kname, kms, kbytes = max(cands, key=lambda c: c[1])
     traffic = load_traffic(f"rmat{args.scale}_ef16_hybrid_p{p}_theta{theta}:{kname}")

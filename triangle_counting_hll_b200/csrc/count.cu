@@ -766,8 +766,14 @@ __global__ void core_mark_kernel(const int32_t* __restrict__ row_ptr, int64_t n_
             }
             for (int32_t i = s + lane; i < e; i += 32) {
                 const int32_t w = __ldg(col + i);
-                if ((uint64_t)(uint32_t)w < (uint64_t)n_nodes) flag[w] = 1;
-                else status |= ST_BAD_KEY;
+                // the core's members recur in many hub lists: read first, and
+                // store only a flag not yet seen set (a stale 0 read just
+                // repeats an idempotent store)
+                if ((uint64_t)(uint32_t)w < (uint64_t)n_nodes) {
+                    if (flag[w] == 0) flag[w] = 1;
+                } else {
+                    status |= ST_BAD_KEY;
+                }
             }
         }
     }
@@ -827,14 +833,27 @@ __device__ __forceinline__ uint32_t plane_key(const int32_t* __restrict__ col, c
     return c >= kPlane ? (uint32_t)(c - kPlane) : 0xFFFFu;
 }
 
-__global__ void core_pad16_kernel(const int32_t* __restrict__ row_ptr, int64_t n_nodes, int64_t nnz,
-                                  const int32_t* __restrict__ col, const int32_t* __restrict__ cidx,
-                                  const int32_t* __restrict__ n_core, int packed, uint16_t* __restrict__ pcol16,
-                                  int2* __restrict__ pl, tchll_count_result* result) {
+// Within each plane the keys are ordered by the shared-memory bank of their
+// bitmap word ((key >> 5) & 31; a list is a set, so order is free): the hub
+// kernel deals consecutive 8-key units to consecutive lanes, so one load
+// instruction then mostly touches distinct banks (simulated on R-MAT: 2.5
+// instead of 3.2 shared-memory wavefronts per load).  A counting sort per
+// row and plane: 8 lanes count the 32 banks in shared memory, scan them and
+// scatter the keys; the order inside a bank is arbitrary.
+__global__ void __launch_bounds__(256) core_pad16_kernel(const int32_t* __restrict__ row_ptr, int64_t n_nodes,
+                                                         int64_t nnz, const int32_t* __restrict__ col,
+                                                         const int32_t* __restrict__ cidx,
+                                                         const int32_t* __restrict__ n_core, int packed,
+                                                         uint16_t* __restrict__ pcol16, int2* __restrict__ pl,
+                                                         tchll_count_result* result) {
+    __shared__ int s_cnt[32][32];  // per 8-lane group: bank counters, then cursors
     const int32_t C = n_core[0];
     if (!packed || C > kCore16Max) return;  // grid-uniform: the 32-bit lists apply
     const int32_t wsplit = n_core[1];       // -1: no plane 1
-    const int sub = threadIdx.x & 7;        // 8 lanes per row, one 16-byte unit each
+    const int lane = threadIdx.x & 31;
+    const int sub = threadIdx.x & 7;        // 8 lanes per row
+    const unsigned gmask = 0xFFu << (lane & 24);
+    int* cnt = s_cnt[threadIdx.x >> 3];
     const int64_t g = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 3;
     const int64_t ng = ((int64_t)gridDim.x * blockDim.x) >> 3;
     uint32_t status = 0;
@@ -857,21 +876,42 @@ __global__ void core_pad16_kernel(const int32_t* __restrict__ row_ptr, int64_t n
         }
         const int32_t lo_units = (P + 7) >> 3, units = lo_units + ((d - P + 7) >> 3);
         const int64_t ps = pad16_start(rs, (int32_t)y);
-        for (int32_t u = sub; u < units; u += 8) {
-            const int plane = u < lo_units ? 0 : 1;
-            const int32_t m0 = plane == 0 ? 8 * u : P + 8 * (u - lo_units);
-            const int32_t end = plane == 0 ? P : d;
-            uint32_t k[8];
+        for (int plane = 0; plane < 2; ++plane) {
+            const int32_t m0 = plane ? P : 0, m1 = plane ? d : P;
+            if (m1 <= m0) continue;  // group-uniform
+            uint16_t* out = pcol16 + ps + (plane ? 8 * (int64_t)lo_units : 0);
+            for (int b = sub; b < 32; b += 8) cnt[b] = 0;
+            __syncwarp(gmask);
+            for (int32_t m = m0 + sub; m < m1; m += 8)
+                atomicAdd(cnt + ((plane_key(col, cidx, n_nodes, rs + m, plane, status) >> 5) & 31u), 1);
+            __syncwarp(gmask);
+            // exclusive scan of the 32 counters, 4 per lane
+            const int c0 = cnt[4 * sub], c1 = cnt[4 * sub + 1], c2 = cnt[4 * sub + 2], c3 = cnt[4 * sub + 3];
+            int incl = c0 + c1 + c2 + c3;
 #pragma unroll
-            for (int t = 0; t < 8; ++t)
-                k[t] = (m0 + t < end) ? plane_key(col, cidx, n_nodes, rs + m0 + t, plane, status) : 0xFFFFu;
-            *reinterpret_cast<uint4*>(pcol16 + ps + 8 * u) =
-                make_uint4(k[0] | (k[1] << 16), k[2] | (k[3] << 16), k[4] | (k[5] << 16), k[6] | (k[7] << 16));
+            for (int o = 1; o < 8; o <<= 1) {
+                const int t = __shfl_up_sync(gmask, incl, o, 8);
+                if (sub >= o) incl += t;
+            }
+            const int ex = incl - (c0 + c1 + c2 + c3);
+            __syncwarp(gmask);
+            cnt[4 * sub] = ex;
+            cnt[4 * sub + 1] = ex + c0;
+            cnt[4 * sub + 2] = ex + c0 + c1;
+            cnt[4 * sub + 3] = ex + c0 + c1 + c2;
+            __syncwarp(gmask);
+            for (int32_t m = m0 + sub; m < m1; m += 8) {
+                const uint32_t k = plane_key(col, cidx, n_nodes, rs + m, plane, status);
+                out[atomicAdd(cnt + ((k >> 5) & 31u), 1)] = (uint16_t)k;
+            }
+            const int32_t nk = m1 - m0;
+            for (int32_t t = nk + sub; t < ((nk + 7) & ~7); t += 8) out[t] = 0xFFFFu;
+            __syncwarp(gmask);  // the counters are reused by the next plane / row
         }
         if (sub == 0) pl[y] = make_int2(lo_units, units);
     }
     status = __reduce_or_sync(FULL, status);
-    if ((threadIdx.x & 31) == 0 && status) atomicOr(&result->status, status);
+    if (lane == 0 && status) atomicOr(&result->status, status);
 }
 
 // Probe lists in core coordinates, padded: 8 lanes per row, one 16-byte
@@ -1814,7 +1854,7 @@ struct Tuning {
     int bitmap_lg = 15;     // hub bitmap buffer: 2^15 bytes = 262,144 core vertices (0: hash tables only)
     int overlap = 1;        // hybrid: HLL pass on a side stream beside the exact pairs
     int packed = 1;         // hub probe lists as 16-bit core indices when the core allows
-    int hll_row_cache_p = 10;  // HLL pass: keep u's register row in registers for p <= this
+    int hll_row_cache_p = 0;   // HLL pass: keep u's register row in registers for p <= this (0: never)
     int hll_lanes = 0;      // HLL pass: lanes per edge (0: chosen by p)
 };
 constexpr int HUB_MIN = 64;       // smallest hub threshold (bounds the segment count)
@@ -1859,10 +1899,11 @@ struct PhaseTimer {
     std::atomic<bool> on{false};
     bool made = false;
     cudaEvent_t ev[4];
-    cudaEvent_t hub_ev[3];  // core pass start, hub kernels start, hub kernels end (inside phase 1)
+    cudaEvent_t hub_ev[4];  // core pass start / end, hub kernels start / end (inside phase 1)
     cudaEvent_t hll_ev[2];  // around the HLL pass when it runs on the side stream
     bool used[3] = {false, false, false};
     bool hub_used = false;
+    bool core_used = false;
     bool hll_split = false;  // phase 2 (HLL) is timed by hll_ev, not ev[2..3]
 };
 static PhaseTimer g_phase;
@@ -1889,6 +1930,7 @@ static void phase_reset(const PhaseScope& ps) {
     if (!ps.active()) return;
     for (int i = 0; i < 3; ++i) g_phase.used[i] = false;
     g_phase.hub_used = false;
+    g_phase.core_used = false;
     g_phase.hll_split = false;
 }
 
@@ -2055,17 +2097,19 @@ static int launch_hll_edges(const CountParams& P, const HybridWs& HW, const Tuni
     H.zst = HW.zst;
     // p <= row_cache_p (with zero masks): contiguous runs per group with u's
     // register row kept in registers, m / 128 lanes per edge (8 16-byte
-    // words of the row per lane).  Otherwise: for p >= 11 the
-    // linear-counting shortcut settles almost every edge from the masks
-    // alone, a pass bound by the latency of its dependent loads: four mask
-    // loads per lane per row, several edges per warp in flight; for p = 9, 10
-    // one mask load per lane; for p <= 8 one lane per edge; without masks
-    // one 16-byte register load per lane per row.  (Measured on R-MAT scale
-    // 22, theta = 256.)  T.hll_lanes > 0 overrides the width.
+    // words of the row per lane; off by default: at 128 registers per
+    // thread too few warps hide the loads).  With zero masks the pass is
+    // bound by the latency of its dependent loads, so narrow groups (more
+    // edges in flight per warp) win: one lane per edge for p <= 10, 4 for
+    // p = 11, 12, 8 above (R-MAT scale 22, theta = 256, beside the exact
+    // pairs: p = 10 14.2 ms per hybrid step with 1 lane against 15.5 with 8;
+    // p = 12 10.7 with 4 against 11.1 with 8; p = 14 14.0 with 8 against
+    // 17.8 with 32).  Without masks one 16-byte register load per lane per
+    // row.  T.hll_lanes > 0 overrides the width.
     const bool crow = H.zm != nullptr && P.p <= T.hll_row_cache_p;
     int width = (1 << P.p) >> 4;
     if (crow) width = (1 << P.p) >> 7;
-    else if (H.zm) width = P.p >= 11 ? H.zst >> 4 : (P.p >= 9 ? H.zst >> 2 : 1);
+    else if (H.zm) width = P.p <= 10 ? 1 : (P.p <= 12 ? 4 : 8);
     if (T.hll_lanes > 0) width = T.hll_lanes;
     if (H.zm) {
         const int64_t rows = P.slot ? P.n_rows : P.n_nodes;
@@ -2141,11 +2185,52 @@ static int grid_rows(int64_t n, int per_cta) {  // one unit of work per 256 / pe
     return (int)(g < 1 ? 1 : (g > cap ? cap : g));
 }
 
+// The hub core pass and kernels use the padded lists when the workspace
+// holds them and 16-byte unit indices fit int.
+static bool hub_pad_usable(const CountParams& P, const CountWs& W) {
+    const int64_t need_pad = pad_capacity(P.n_nodes, P.nnz);
+    return W.pcol != nullptr && need_pad <= W.pcap && need_pad <= (int64_t)INT32_MAX;
+}
+
+// The hub core pass (needs the hub histogram W.cnth only, so it may run on a
+// second stream beside the pair scatter and the short-list pairs): core
+// flags, their scan, core indices, then the padded lists, packed 16-bit when
+// the core allows it, else 32-bit (each pad kernel checks the core size on
+// the device).
+static int launch_core_pass(const CountParams& P, const CountWs& W, const Tuning& T, const PhaseScope& ps,
+                            cudaStream_t st) {
+    if (!hub_pad_usable(P, W)) return TCHLL_OK;
+    if (ps.active()) {
+        cudaEventRecord(g_phase.hub_ev[0], st);
+        g_phase.core_used = true;
+    }
+    const int64_t N = P.n_nodes + 1;
+    TCHLL_CUDA(cudaMemsetAsync(W.cflag, 0, sizeof(int32_t) * N, st));
+    core_mark_kernel<<<grid_rows(P.n_nodes, 256), 256, 0, st>>>(P.row_ptr, P.n_nodes, P.nnz, P.col_idx, W.cnth,
+                                                                 W.cflag, P.result);
+    TCHLL_CHECK_LAUNCH("core_mark_kernel");
+    size_t tb = W.tmp_bytes;
+    TCHLL_CUDA(cub::DeviceScan::ExclusiveSum(W.tmp, tb, W.cflag, W.cpos, (int)N, st));
+    count_launch();
+    TCHLL_CUDA(cudaMemsetAsync(W.ncore + 1, 0xFF, sizeof(int32_t), st));
+    core_index_kernel<<<grid_rows(N, 256), 256, 0, st>>>(W.cflag, W.cpos, P.n_nodes, W.ncore);
+    TCHLL_CHECK_LAUNCH("core_index_kernel");
+    core_pad16_kernel<<<grid_rows(P.n_nodes, 32), 256, 0, st>>>(P.row_ptr, P.n_nodes, P.nnz, P.col_idx, W.cflag,
+                                                                W.ncore, T.packed, reinterpret_cast<uint16_t*>(W.pcol),
+                                                                W.pl, P.result);
+    TCHLL_CHECK_LAUNCH("core_pad16_kernel");
+    core_pad_kernel<<<grid_rows(P.n_nodes, 32), 256, 0, st>>>(P.row_ptr, P.n_nodes, P.nnz, P.col_idx, W.cflag,
+                                                              W.ncore, T.packed, W.pcol, P.result);
+    TCHLL_CHECK_LAUNCH("core_pad_kernel");
+    if (ps.active()) cudaEventRecord(g_phase.hub_ev[1], st);
+    return TCHLL_OK;
+}
+
 // The hub pairs: one CTA per segment at a time, persistent grid.  With the
-// padded lists in the workspace: the core pass (flags, scan, indices,
-// filtered lists), then the bitmap kernel, then the hash kernel, which
-// returns at once when the bitmap kernel could hold the core.  Without them
-// (a small workspace): the hash kernel over the raw lists.
+// padded lists (the core pass done before, on this stream or waited for):
+// the packed bitmap kernel, the 32-bit bitmap kernel, then the hash kernel;
+// each but the one the core size selects returns at once.  Without them (a
+// small workspace): the hash kernel over the raw lists.
 static int launch_hub(const CountParams& P, const CountWs& W, const Tuning& T, const PhaseScope& ps, cudaStream_t st,
                       bool batched = false) {
     HubParams H{};
@@ -2161,40 +2246,15 @@ static int launch_hub(const CountParams& P, const CountWs& W, const Tuning& T, c
     H.seg_ctr = W.ctr + 3;
     H.hub_lg = T.hub_lg;
     H.result = P.result;
-    // padded lists in core coordinates when the workspace holds them and quad
-    // indices fit int
-    const int64_t need_pad = pad_capacity(P.n_nodes, P.nnz);
-    const bool pad = W.pcol != nullptr && need_pad <= W.pcap && need_pad <= (int64_t)INT32_MAX;
-    if (ps.active()) cudaEventRecord(g_phase.hub_ev[0], st);
+    const bool pad = hub_pad_usable(P, W);
     if (pad) {
-        const int64_t N = P.n_nodes + 1;
-        TCHLL_CUDA(cudaMemsetAsync(W.cflag, 0, sizeof(int32_t) * N, st));
-        core_mark_kernel<<<grid_rows(P.n_nodes, 256), 256, 0, st>>>(P.row_ptr, P.n_nodes, P.nnz, P.col_idx, W.cnth,
-                                                                     W.cflag, P.result);
-        TCHLL_CHECK_LAUNCH("core_mark_kernel");
-        size_t tb = W.tmp_bytes;
-        TCHLL_CUDA(cub::DeviceScan::ExclusiveSum(W.tmp, tb, W.cflag, W.cpos, (int)N, st));
-        count_launch();
-        TCHLL_CUDA(cudaMemsetAsync(W.ncore + 1, 0xFF, sizeof(int32_t), st));
-        core_index_kernel<<<grid_rows(N, 256), 256, 0, st>>>(W.cflag, W.cpos, P.n_nodes, W.ncore);
-        TCHLL_CHECK_LAUNCH("core_index_kernel");
-        // packed 16-bit lists when the core allows it, else 32-bit lists
-        // (each kernel checks the core size on the device)
-        core_pad16_kernel<<<grid_rows(P.n_nodes, 32), 256, 0, st>>>(P.row_ptr, P.n_nodes, P.nnz, P.col_idx,
-                                                                    W.cflag, W.ncore, T.packed,
-                                                                    reinterpret_cast<uint16_t*>(W.pcol), W.pl,
-                                                                    P.result);
-        TCHLL_CHECK_LAUNCH("core_pad16_kernel");
-        core_pad_kernel<<<grid_rows(P.n_nodes, 32), 256, 0, st>>>(P.row_ptr, P.n_nodes, P.nnz, P.col_idx, W.cflag,
-                                                                  W.ncore, T.packed, W.pcol, P.result);
-        TCHLL_CHECK_LAUNCH("core_pad_kernel");
         H.pcol = W.pcol;
         H.cidx = W.cflag;
         H.n_core = W.ncore;
         H.pl = W.pl;
         H.packed = T.packed;
     }
-    if (ps.active()) cudaEventRecord(g_phase.hub_ev[1], st);
+    if (ps.active()) cudaEventRecord(g_phase.hub_ev[2], st);
     if (pad && T.packed) {
         const size_t smem = 16384;
         auto kern = T.hub_unroll == 4 ? hub_bitmap16_kernel<4> : hub_bitmap16_kernel<2>;
@@ -2238,7 +2298,7 @@ static int launch_hub(const CountParams& P, const CountWs& W, const Tuning& T, c
     kern<<<sm_count() * bps, 256, smem, st>>>(H);
     TCHLL_CHECK_LAUNCH("hub_count_kernel");
     if (ps.active()) {
-        cudaEventRecord(g_phase.hub_ev[2], st);
+        cudaEventRecord(g_phase.hub_ev[3], st);
         g_phase.hub_used = true;
     }
     return TCHLL_OK;
@@ -2247,15 +2307,6 @@ static int launch_hub(const CountParams& P, const CountWs& W, const Tuning& T, c
 // Hub path in use: pairs on, and 16-byte aligned col_idx (quad loads).
 static int hub_threshold(const CountParams& P, const Tuning& T) {
     return (T.hub > 0 && (uintptr_t)P.col_idx % 16 == 0) ? T.hub : 0;
-}
-
-// Build the grouped (x, y) pair list of the exact edges into Q.
-template <bool HYB>
-static int build_pairs(const CountParams& P, const CountWs& W, int hub, int hub_seg, CountParams& Q,
-                       cudaStream_t st) {
-    int rc = pairs_hist_scan<HYB>(P, W, hub, hub_seg, st);
-    if (rc) return rc;
-    return pairs_scatter<HYB>(P, W, hub, Q, st);
 }
 
 // A second stream per device for work that overlaps the caller's stream: the
@@ -2269,7 +2320,7 @@ static int build_pairs(const CountParams& P, const CountWs& W, int hub, int hub_
 // capture: the first call of a process is never captured by this package).
 struct SideStream {
     cudaStream_t s = nullptr;
-    cudaEvent_t fork = nullptr, join = nullptr;
+    cudaEvent_t fork = nullptr, mid = nullptr, join = nullptr;
     std::mutex mu;
 };
 static SideStream g_side[kMaxDevices];
@@ -2288,6 +2339,7 @@ class SideFork {
             if (S.s == nullptr) {
                 TCHLL_CUDA(cudaStreamCreateWithFlags(&S.s, cudaStreamNonBlocking));
                 TCHLL_CUDA(cudaEventCreateWithFlags(&S.fork, cudaEventDisableTiming));
+                TCHLL_CUDA(cudaEventCreateWithFlags(&S.mid, cudaEventDisableTiming));
                 TCHLL_CUDA(cudaEventCreateWithFlags(&S.join, cudaEventDisableTiming));
             }
         }
@@ -2299,6 +2351,16 @@ class SideFork {
         return TCHLL_OK;
     }
     cudaStream_t stream() const { return side_->s; }
+    // Marks the side stream's work so far; wait_mark makes the caller's
+    // stream wait for it (once per fork).
+    int mark() {
+        TCHLL_CUDA(cudaEventRecord(side_->mid, side_->s));
+        return TCHLL_OK;
+    }
+    int wait_mark() {
+        TCHLL_CUDA(cudaStreamWaitEvent(caller_, side_->mid, 0));
+        return TCHLL_OK;
+    }
     // Joins: the caller's stream waits for everything enqueued on the side
     // stream so far.  Safe to call more than once.
     int end() {
@@ -2362,16 +2424,33 @@ static int run_count(CountParams P, int mode, bool details, void* ws, size_t ws_
         case MODE_EXACT:
             P.work = W.ctr;
             if (pairs) {
+                // after the histogram, the hub core pass runs on the side
+                // stream beside the pair scatter and the short-list pairs;
+                // the hub kernels wait for it
                 const int hub = hub_threshold(P, T);
                 phase_mark(ps, 0, st);
-                rc = build_pairs<false>(P, W, hub, T.hub_seg, Q, st);
+                rc = pairs_hist_scan<false>(P, W, hub, T.hub_seg, st);
+                if (rc) return rc;
+                SideFork fork;
+                const bool side = hub > 0 && T.overlap && hub_pad_usable(P, W);
+                if (side) {
+                    rc = fork.begin(st);
+                    if (rc == TCHLL_OK) rc = launch_core_pass(P, W, T, ps, fork.stream());
+                    if (rc == TCHLL_OK) rc = fork.mark();
+                    if (rc) return rc;
+                }
+                rc = pairs_scatter<false>(P, W, hub, Q, st);
                 if (rc) return rc;
                 phase_mark(ps, 1, st);
                 rc = launch_count<MODE_EXACT>(Q, T, false, st);
-                if (rc == TCHLL_OK && hub > 0) rc = launch_hub(P, W, T, ps, st);
+                if (rc == TCHLL_OK && hub > 0) {
+                    rc = side ? fork.wait_mark() : launch_core_pass(P, W, T, ps, st);
+                    if (rc == TCHLL_OK) rc = launch_hub(P, W, T, ps, st);
+                }
                 phase_mark(ps, 2, st);
+                const int rj = fork.end();
                 phase_used(ps, 0, 1);
-                return rc;
+                return rc ? rc : rj;
             }
             phase_mark(ps, 1, st);
             rc = launch_count<MODE_EXACT>(P, T, details, st);
@@ -2404,12 +2483,20 @@ static int run_count(CountParams P, int mode, bool details, void* ws, size_t ws_
                 phase_mark(ps, 0, st);
                 rc = pairs_hist_scan<true>(P, W, hub, T.hub_seg, st);
                 if (rc) return rc;
+                // side stream: the hub core pass first (the hub kernels wait
+                // for it), then the HLL pass
                 SideFork fork;
                 cudaStream_t hst = st;
+                const bool core_side = hub > 0 && T.overlap && hub_pad_usable(P, W);
                 if (T.overlap) {
                     rc = fork.begin(st);
                     if (rc) return rc;
                     hst = fork.stream();
+                    if (core_side) {
+                        rc = launch_core_pass(P, W, T, ps, hst);
+                        if (rc == TCHLL_OK) rc = fork.mark();
+                        if (rc) return rc;
+                    }
                 }
                 if (ps.active()) cudaEventRecord(g_phase.hll_ev[0], hst);
                 rc = launch_hll_edges(P, HW, T, hst);
@@ -2422,7 +2509,8 @@ static int run_count(CountParams P, int mode, bool details, void* ws, size_t ws_
                 rc = launch_count<MODE_EXACT>(Q, T, false, st);
                 if (rc) return rc;
                 if (hub > 0) {
-                    rc = launch_hub(P, W, T, ps, st);
+                    rc = core_side ? fork.wait_mark() : launch_core_pass(P, W, T, ps, st);
+                    if (rc == TCHLL_OK) rc = launch_hub(P, W, T, ps, st);
                     if (rc) return rc;
                 }
                 phase_mark(ps, 2, st);
@@ -2670,13 +2758,14 @@ TCHLL_EXPORT int tchll_set_phase_timing(int32_t enable) {
     std::lock_guard<std::mutex> lock(g_phase_mu);
     if (enable && !g_phase.made) {
         for (int i = 0; i < 4; ++i) TCHLL_CUDA(cudaEventCreate(&g_phase.ev[i]));
-        for (int i = 0; i < 3; ++i) TCHLL_CUDA(cudaEventCreate(&g_phase.hub_ev[i]));
+        for (int i = 0; i < 4; ++i) TCHLL_CUDA(cudaEventCreate(&g_phase.hub_ev[i]));
         for (int i = 0; i < 2; ++i) TCHLL_CUDA(cudaEventCreate(&g_phase.hll_ev[i]));
         g_phase.made = true;
     }
     g_phase.on = enable != 0;
     for (int i = 0; i < 3; ++i) g_phase.used[i] = false;
     g_phase.hub_used = false;
+    g_phase.core_used = false;
     g_phase.hll_split = false;
     return TCHLL_OK;
 }
@@ -2704,9 +2793,9 @@ TCHLL_EXPORT int tchll_phase_hub_ms(float* ms2) {
     std::lock_guard<std::mutex> lock(g_phase_mu);
     ms2[0] = ms2[1] = -1.0f;
     if (!g_phase.on || !g_phase.made || !g_phase.hub_used) return TCHLL_OK;
-    TCHLL_CUDA(cudaEventSynchronize(g_phase.hub_ev[2]));
-    TCHLL_CUDA(cudaEventElapsedTime(&ms2[0], g_phase.hub_ev[1], g_phase.hub_ev[2]));
-    TCHLL_CUDA(cudaEventElapsedTime(&ms2[1], g_phase.hub_ev[0], g_phase.hub_ev[1]));
+    TCHLL_CUDA(cudaEventSynchronize(g_phase.hub_ev[3]));
+    TCHLL_CUDA(cudaEventElapsedTime(&ms2[0], g_phase.hub_ev[2], g_phase.hub_ev[3]));
+    if (g_phase.core_used) TCHLL_CUDA(cudaEventElapsedTime(&ms2[1], g_phase.hub_ev[0], g_phase.hub_ev[1]));
     return TCHLL_OK;
 }
 
@@ -3004,7 +3093,8 @@ static int run_batch(CountParams P, bool hybrid, const int32_t* vbase, int64_t n
     rc = launch_count<MODE_EXACT>(Q, T, false, st);
     if (rc) return rc;
     if (hub > 0) {
-        rc = launch_hub(P, B.cw, T, ps, st, true);
+        rc = launch_core_pass(P, B.cw, T, ps, st);
+        if (rc == TCHLL_OK) rc = launch_hub(P, B.cw, T, ps, st, true);
         if (rc) return rc;
     }
     phase_mark(ps, 2, st);
