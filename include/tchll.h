@@ -165,13 +165,16 @@ int tchll_get_count_hub(int32_t* out4 /* host */);
  * hold 16-bit core indices (two planes) and the bitmap takes 16 KB; else,
  * when the core fits 8 * 2^bitmap_log2 bits (minus 32), 32-bit lists and a
  * bitmap of that size; else hash tables.  bitmap_log2 0 turns the 32-bit
- * bitmap off; otherwise in [10, 17].  overlap != 0 runs a hybrid count's HLL
- * pass on a second stream beside the exact pairs (joined before the call
- * returns).  out3 receives the three values.  Results are identical for
- * every setting.  These kernels read col_idx values as vertex indices: a
- * value outside [0, n_nodes) is reported as TCHLL_STATUS_BAD_KEY. */
-int tchll_set_count_core(int32_t bitmap_log2, int32_t overlap, int32_t packed);
-int tchll_get_count_core(int32_t* out3 /* host */);
+ * bitmap off; otherwise in [10, 17].  overlap != 0 runs the hub core pass
+ * and a hybrid count's HLL pass on a second stream beside the exact pairs
+ * (joined before the call returns).  bank_sort != 0 orders each packed
+ * list's keys by the shared-memory bank of their bitmap word (fewer bank
+ * conflicts in the hub kernel, a slower core pass).  out4 receives the four
+ * values.  Results are identical for every setting.  These kernels read
+ * col_idx values as vertex indices: a value outside [0, n_nodes) is
+ * reported as TCHLL_STATUS_BAD_KEY. */
+int tchll_set_count_core(int32_t bitmap_log2, int32_t overlap, int32_t packed, int32_t bank_sort);
+int tchll_get_count_core(int32_t* out4 /* host */);
 
 /* HLL pass of the hybrid counts (with the zero masks in the workspace):
  * for p <= row_cache_max_p each group of lanes takes a contiguous run of the

@@ -355,9 +355,10 @@ def test_hub_core_bitmap_hash_and_overlap_match_oracle(tchll, oracle, dev):
     blocks = []
     try:
         for hub, blg, ov, pk in ((128, 15, 1, 1), (128, 15, 1, 0), (128, 0, 1, 0), (64, 10, 0, 0), (64, 15, 0, 1),
-                                 (128, 12, 1, 0), (200, 17, 1, 0), (64, 0, 0, 1)):
+                                 (128, 12, 1, 0), (200, 17, 1, 0), (64, 0, 0, 1), (128, 0, 1, 2), (64, 0, 0, 2)):
+            # pk 2: packed lists ordered by bitmap bank
             core.set_count_tuning(base["chunk"], base["slots_log2"], base["tiny"], base["blocks_per_sm"], hub=hub,
-                                  bitmap_lg=blg, overlap=bool(ov), packed=bool(pk))
+                                  bitmap_lg=blg, overlap=bool(ov), packed=bool(pk), bank_sort=pk == 2)
             assert core.get_count_tuning()["bitmap_lg"] == blg
             assert _exact(core, g) == want, (hub, blg, ov, pk)
             res, _ = core.hybrid_count_compact_tensors(g.row_ptr, g.col_idx, g.edge_u, g.edge_v, g.degrees, rows,

@@ -72,7 +72,7 @@ SIGNATURES = {
     "tchll_get_count_tuning": (C.c_int, [_P]),
     "tchll_set_count_hub": (C.c_int, [_I32, _I32, _I32, _I32]),
     "tchll_get_count_hub": (C.c_int, [_P]),
-    "tchll_set_count_core": (C.c_int, [_I32, _I32, _I32]),
+    "tchll_set_count_core": (C.c_int, [_I32, _I32, _I32, _I32]),
     "tchll_get_count_core": (C.c_int, [_P]),
     "tchll_set_hll_pass": (C.c_int, [_I32, _I32]),
     "tchll_get_hll_pass": (C.c_int, [_P]),

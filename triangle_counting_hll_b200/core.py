@@ -246,12 +246,12 @@ def hybrid_count_compact_tensors(row_ptr, col_idx, edge_u, edge_v, degrees, rows
     return res, pe
 
 
-def set_count_tuning(chunk: int = 256, slots_log2: int = 11, tiny: int = 16, blocks_per_sm: int = 0,
+def set_count_tuning(chunk: int = 256, slots_log2: int = 10, tiny: int = 16, blocks_per_sm: int = 0,
                      warps: Optional[int] = None, pairs: Optional[bool] = None,
                      sparse: Optional[bool] = None, hub: Optional[int] = None, hub_seg: Optional[int] = None,
                      hub_lg: Optional[int] = None, hub_unroll: Optional[int] = None,
                      bitmap_lg: Optional[int] = None, overlap: Optional[bool] = None,
-                     packed: Optional[bool] = None,
+                     packed: Optional[bool] = None, bank_sort: Optional[bool] = None,
                      hll_row_cache_p: Optional[int] = None, hll_lanes: Optional[int] = None) -> None:
     """Launch shape of the counting kernels (results do not depend on it).
     hub / hub_seg / hub_lg / hub_unroll: threshold on d+(x) above which a pair
@@ -259,7 +259,8 @@ def set_count_tuning(chunk: int = 256, slots_log2: int = 11, tiny: int = 16, blo
     hash-table slots, probe loads in flight per lane.  bitmap_lg: log2 bytes
     of the 32-bit hub bitmap buffer (0: off); overlap: hybrid HLL pass on a
     second stream beside the exact pairs; packed: 16-bit hub probe lists when
-    the core has at most 131,070 vertices.  hll_row_cache_p / hll_lanes:
+    the core has at most 131,070 vertices; bank_sort: packed lists ordered by
+    bitmap bank.  hll_row_cache_p / hll_lanes:
     the HLL pass's one-pass threshold on p and lanes per edge (0: by p)."""
     L = load()
     cur = get_count_tuning()
@@ -267,7 +268,8 @@ def set_count_tuning(chunk: int = 256, slots_log2: int = 11, tiny: int = 16, blo
                                int(cur["hll_lanes"] if hll_lanes is None else hll_lanes)))
     check(L.tchll_set_count_core(int(cur["bitmap_lg"] if bitmap_lg is None else bitmap_lg),
                                  int(cur["overlap"] if overlap is None else bool(overlap)),
-                                 int(cur["packed"] if packed is None else bool(packed))))
+                                 int(cur["packed"] if packed is None else bool(packed)),
+                                 int(cur["bank_sort"] if bank_sort is None else bool(bank_sort))))
     check(L.tchll_set_count_hub(int(cur["hub"] if hub is None else hub),
                                 int(cur["hub_seg"] if hub_seg is None else hub_seg),
                                 int(cur["hub_lg"] if hub_lg is None else hub_lg),
@@ -286,13 +288,14 @@ def get_count_tuning() -> dict:
     check(load().tchll_get_count_tuning(C.cast(out, C.c_void_p)))
     hub = (C.c_int32 * 4)()
     check(load().tchll_get_count_hub(C.cast(hub, C.c_void_p)))
-    co = (C.c_int32 * 3)()
+    co = (C.c_int32 * 4)()
     check(load().tchll_get_count_core(C.cast(co, C.c_void_p)))
     hp = (C.c_int32 * 2)()
     check(load().tchll_get_hll_pass(C.cast(hp, C.c_void_p)))
     return {"chunk": out[0], "slots_log2": out[1], "tiny": out[2], "blocks_per_sm": out[3], "warps": out[4],
             "pairs": out[5], "sparse": out[6], "hub": hub[0], "hub_seg": hub[1], "hub_lg": hub[2],
-            "hub_unroll": hub[3], "bitmap_lg": co[0], "overlap": co[1], "packed": co[2], "hll_row_cache_p": hp[0],
+            "hub_unroll": hub[3], "bitmap_lg": co[0], "overlap": co[1], "packed": co[2], "bank_sort": co[3],
+            "hll_row_cache_p": hp[0],
             "hll_lanes": hp[1]}
 
 

@@ -375,7 +375,7 @@ __device__ __forceinline__ void publish(tchll_count_result* R, uint64_t acc, U12
 }
 
 template <int MODE, bool VEC, bool DETAILS>
-__global__ void __launch_bounds__(256, 3) count_kernel(const CountParams P) {
+__global__ void __launch_bounds__(256, 4) count_kernel(const CountParams P) {
     extern __shared__ __align__(16) int32_t smem[];
     const int lane = threadIdx.x & 31;
     const int wid = threadIdx.x >> 5;
@@ -742,38 +742,40 @@ __device__ __forceinline__ int64_t pad_start(int32_t rs, int32_t y) {
     return (((int64_t)rs + 3) & ~(int64_t)3) + 8 * (int64_t)y;
 }
 
-// flag[w] = 1 for every w in N+(x) of every x with hub pairs (cnth[x] > 0).
-// One warp per 32 consecutive x; the warp stores the flags of each hub x's
-// list together.  Values outside [0, n_nodes) are reported, not stored.
+// flag[w] = 1 for every w in N+(x) of every x with hub pairs: one warp per
+// hub segment (a segment names its x; an x with several segments is marked
+// more than once, idempotently).  Going by segments rather than by vertex id
+// keeps the warps balanced: hub vertices cluster at low ids in R-MAT graphs.
+// Values outside [0, n_nodes) are reported, not stored.
 __global__ void core_mark_kernel(const int32_t* __restrict__ row_ptr, int64_t n_nodes, int64_t nnz,
-                                 const int32_t* __restrict__ col, const int32_t* __restrict__ cnth, int32_t* flag,
+                                 const int32_t* __restrict__ col, const HubSeg* __restrict__ segs,
+                                 const unsigned long long* __restrict__ n_segs, int64_t max_segs, int32_t* flag,
                                  tchll_count_result* result) {
     const int lane = threadIdx.x & 31;
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t nseg = min((int64_t)*n_segs, max_segs);
     uint32_t status = 0;
-    for (int64_t x0 = warp * 32; x0 < n_nodes; x0 += nwarps * 32) {
-        const int64_t x = x0 + lane;
-        const bool hub = x < n_nodes && __ldg(cnth + x) > 0;
-        unsigned b = __ballot_sync(FULL, hub);
-        while (b) {
-            const int j = __ffs(b) - 1;
-            b &= b - 1;
-            const int32_t s = __ldg(row_ptr + x0 + j), e = __ldg(row_ptr + x0 + j + 1);
-            if (s < 0 || e < s || (int64_t)e > nnz) {  // warp-uniform
-                status |= ST_BAD_ROW;
-                continue;
-            }
-            for (int32_t i = s + lane; i < e; i += 32) {
-                const int32_t w = __ldg(col + i);
-                // the core's members recur in many hub lists: read first, and
-                // store only a flag not yet seen set (a stale 0 read just
-                // repeats an idempotent store)
-                if ((uint64_t)(uint32_t)w < (uint64_t)n_nodes) {
-                    if (flag[w] == 0) flag[w] = 1;
-                } else {
-                    status |= ST_BAD_KEY;
-                }
+    for (int64_t sg = warp; sg < nseg; sg += nwarps) {
+        const int32_t x = segs[sg].x;
+        if (x < 0 || (int64_t)x >= n_nodes) {  // warp-uniform; cannot happen
+            status |= ST_BAD_EDGE;
+            continue;
+        }
+        const int32_t s = __ldg(row_ptr + x), e = __ldg(row_ptr + x + 1);
+        if (s < 0 || e < s || (int64_t)e > nnz) {
+            status |= ST_BAD_ROW;
+            continue;
+        }
+        for (int32_t i = s + lane; i < e; i += 32) {
+            const int32_t w = __ldg(col + i);
+            // the core's members recur in many hub lists: read first, and
+            // store only a flag not yet seen set (a stale 0 read just
+            // repeats an idempotent store)
+            if ((uint64_t)(uint32_t)w < (uint64_t)n_nodes) {
+                if (flag[w] == 0) flag[w] = 1;
+            } else {
+                status |= ST_BAD_KEY;
             }
         }
     }
@@ -781,9 +783,6 @@ __global__ void core_mark_kernel(const int32_t* __restrict__ row_ptr, int64_t n_
     if (lane == 0 && status) atomicOr(&result->status, status);
 }
 
-// After the exclusive scan pos = scan(flag) over n_nodes + 1 entries (flag[n]
-// = 0): cidx[w] = pos[w] for flagged w, else -1 (written over flag), and
-// *n_core = pos[n_nodes].
 // Packed probe lists hold a core index in 16 bits plus a plane: plane 0 the
 // indices below kPlane, plane 1 the others minus kPlane, each plane padded
 // with 0xFFFF.  In the bitmap, core index c sits at bit c (plane 0) or c + 1
@@ -844,8 +843,8 @@ __global__ void __launch_bounds__(256) core_pad16_kernel(const int32_t* __restri
                                                          int64_t nnz, const int32_t* __restrict__ col,
                                                          const int32_t* __restrict__ cidx,
                                                          const int32_t* __restrict__ n_core, int packed,
-                                                         uint16_t* __restrict__ pcol16, int2* __restrict__ pl,
-                                                         tchll_count_result* result) {
+                                                         int bank_sort, uint16_t* __restrict__ pcol16,
+                                                         int2* __restrict__ pl, tchll_count_result* result) {
     __shared__ int s_cnt[32][32];  // per 8-lane group: bank counters, then cursors
     const int32_t C = n_core[0];
     if (!packed || C > kCore16Max) return;  // grid-uniform: the 32-bit lists apply
@@ -876,6 +875,21 @@ __global__ void __launch_bounds__(256) core_pad16_kernel(const int32_t* __restri
         }
         const int32_t lo_units = (P + 7) >> 3, units = lo_units + ((d - P + 7) >> 3);
         const int64_t ps = pad16_start(rs, (int32_t)y);
+        if (!bank_sort) {  // list order: one 16-byte unit per lane
+            for (int32_t u = sub; u < units; u += 8) {
+                const int plane = u < lo_units ? 0 : 1;
+                const int32_t m0 = plane == 0 ? 8 * u : P + 8 * (u - lo_units);
+                const int32_t end = plane == 0 ? P : d;
+                uint32_t k[8];
+#pragma unroll
+                for (int t = 0; t < 8; ++t)
+                    k[t] = (m0 + t < end) ? plane_key(col, cidx, n_nodes, rs + m0 + t, plane, status) : 0xFFFFu;
+                *reinterpret_cast<uint4*>(pcol16 + ps + 8 * u) =
+                    make_uint4(k[0] | (k[1] << 16), k[2] | (k[3] << 16), k[4] | (k[5] << 16), k[6] | (k[7] << 16));
+            }
+            if (sub == 0) pl[y] = make_int2(lo_units, units);
+            continue;
+        }
         for (int plane = 0; plane < 2; ++plane) {
             const int32_t m0 = plane ? P : 0, m1 = plane ? d : P;
             if (m1 <= m0) continue;  // group-uniform
@@ -1841,7 +1855,7 @@ __global__ void __launch_bounds__(256, CROW ? 2 : (CACHE ? 3 : 4)) hll_edges_ker
 // ---------------------------------------------------------------- host ------
 struct Tuning {
     int chunk = 256;
-    int slots_log2 = 11;    // 2048 slots = 8 KB per warp
+    int slots_log2 = 10;    // 1024 slots = 4 KB per warp: a table side of up to 128 keys at load <= 1/8
     int tiny = 16;
     int blocks_per_sm = 0;  // 0: occupancy maximum
     int warps = 8;          // warps per CTA
@@ -1854,6 +1868,7 @@ struct Tuning {
     int bitmap_lg = 15;     // hub bitmap buffer: 2^15 bytes = 262,144 core vertices (0: hash tables only)
     int overlap = 1;        // hybrid: HLL pass on a side stream beside the exact pairs
     int packed = 1;         // hub probe lists as 16-bit core indices when the core allows
+    int bank_sort = 0;      // packed lists ordered by bitmap bank within each plane
     int hll_row_cache_p = 0;   // HLL pass: keep u's register row in registers for p <= this (0: never)
     int hll_lanes = 0;      // HLL pass: lanes per edge (0: chosen by p)
 };
@@ -2206,8 +2221,8 @@ static int launch_core_pass(const CountParams& P, const CountWs& W, const Tuning
     }
     const int64_t N = P.n_nodes + 1;
     TCHLL_CUDA(cudaMemsetAsync(W.cflag, 0, sizeof(int32_t) * N, st));
-    core_mark_kernel<<<grid_rows(P.n_nodes, 256), 256, 0, st>>>(P.row_ptr, P.n_nodes, P.nnz, P.col_idx, W.cnth,
-                                                                 W.cflag, P.result);
+    core_mark_kernel<<<sm_count() * 8, 256, 0, st>>>(P.row_ptr, P.n_nodes, P.nnz, P.col_idx, W.segs, W.ctr + 2,
+                                                      W.max_segs, W.cflag, P.result);
     TCHLL_CHECK_LAUNCH("core_mark_kernel");
     size_t tb = W.tmp_bytes;
     TCHLL_CUDA(cub::DeviceScan::ExclusiveSum(W.tmp, tb, W.cflag, W.cpos, (int)N, st));
@@ -2216,8 +2231,8 @@ static int launch_core_pass(const CountParams& P, const CountWs& W, const Tuning
     core_index_kernel<<<grid_rows(N, 256), 256, 0, st>>>(W.cflag, W.cpos, P.n_nodes, W.ncore);
     TCHLL_CHECK_LAUNCH("core_index_kernel");
     core_pad16_kernel<<<grid_rows(P.n_nodes, 32), 256, 0, st>>>(P.row_ptr, P.n_nodes, P.nnz, P.col_idx, W.cflag,
-                                                                W.ncore, T.packed, reinterpret_cast<uint16_t*>(W.pcol),
-                                                                W.pl, P.result);
+                                                                W.ncore, T.packed, T.bank_sort,
+                                                                reinterpret_cast<uint16_t*>(W.pcol), W.pl, P.result);
     TCHLL_CHECK_LAUNCH("core_pad16_kernel");
     core_pad_kernel<<<grid_rows(P.n_nodes, 32), 256, 0, st>>>(P.row_ptr, P.n_nodes, P.nnz, P.col_idx, W.cflag,
                                                               W.ncore, T.packed, W.pcol, P.result);
@@ -2703,22 +2718,24 @@ TCHLL_EXPORT int tchll_get_count_hub(int32_t* out4) {
     return TCHLL_OK;
 }
 
-TCHLL_EXPORT int tchll_set_count_core(int32_t bitmap_log2, int32_t overlap, int32_t packed) {
+TCHLL_EXPORT int tchll_set_count_core(int32_t bitmap_log2, int32_t overlap, int32_t packed, int32_t bank_sort) {
     std::lock_guard<std::mutex> lock(g_tuning_mu);
     TCHLL_ARG(bitmap_log2 == 0 || (bitmap_log2 >= 10 && bitmap_log2 <= 17),
               "bitmap_log2 must be 0 (hash tables only) or in [10, 17] (1 KB .. 128 KB of shared memory)");
     g_tuning.bitmap_lg = bitmap_log2;
     g_tuning.overlap = overlap ? 1 : 0;
     g_tuning.packed = packed ? 1 : 0;
+    g_tuning.bank_sort = bank_sort ? 1 : 0;
     return TCHLL_OK;
 }
 
-TCHLL_EXPORT int tchll_get_count_core(int32_t* out3) {
-    TCHLL_ARG(out3 != nullptr, "null output");
+TCHLL_EXPORT int tchll_get_count_core(int32_t* out4) {
+    TCHLL_ARG(out4 != nullptr, "null output");
     const Tuning T = tuning_snapshot();
-    out3[0] = T.bitmap_lg;
-    out3[1] = T.overlap;
-    out3[2] = T.packed;
+    out4[0] = T.bitmap_lg;
+    out4[1] = T.overlap;
+    out4[2] = T.packed;
+    out4[3] = T.bank_sort;
     return TCHLL_OK;
 }
 

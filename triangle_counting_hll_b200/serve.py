@@ -180,25 +180,37 @@ class _BuildWorker(threading.Thread):
             job = self.inbox.get()
             if job is None:
                 return
-            out, exc = [], None
-            try:
-                with torch.cuda.stream(self.stream):
-                    for key, req, csr in job:
-                        if csr is None:  # a new graph
-                            u, v = generate_edges(req, self.dev)
-                            csr = core.csr_from_edges(u, v, device=self.dev)
-                            del u, v
-                            sk = None
-                            if req.mode == "hybrid" and csr.n_edges >= self.big_edges:
-                                sk = _compact_sketches(csr, req)
-                            out.append((key, csr, sk))
-                        else:  # sketches of a resident large graph
-                            out.append((key, None, _compact_sketches(csr, req)))
-                    ev = torch.cuda.Event()
-                    ev.record(self.stream)
-            except Exception as e:  # reported with the job's queries
-                exc, ev = e, None
-            self.outbox.put((job, out, ev, exc))
+            self.outbox.put(self.build(job))
+
+    def build(self, job):
+        """One build job on the build stream -> (job, built, event, error)."""
+        out, exc = [], None
+        try:
+            with torch.cuda.stream(self.stream):
+                for key, req, csr in job:
+                    if csr is None:  # a new graph
+                        u, v = generate_edges(req, self.dev)
+                        csr = core.csr_from_edges(u, v, device=self.dev)
+                        del u, v
+                        sk = None
+                        if req.mode == "hybrid" and csr.n_edges >= self.big_edges:
+                            sk = _compact_sketches(csr, req)
+                        out.append((key, csr, sk))
+                    else:  # sketches of a resident large graph
+                        out.append((key, None, _compact_sketches(csr, req)))
+                ev = torch.cuda.Event()
+                ev.record(self.stream)
+        except Exception as e:  # reported with the job's queries
+            exc, ev = e, None
+        return job, out, ev, exc
+
+    def submit(self, job) -> None:
+        """Queue a job for the thread, or, when the thread is not running
+        (inline serving), build it now on the calling thread."""
+        if self.is_alive():
+            self.inbox.put(job)
+        else:
+            self.outbox.put(self.build(job))
 
 
 def _compact_sketches(csr: core.DeviceCSR, req: Request):
@@ -213,8 +225,9 @@ class Server:
     docstring."""
 
     def __init__(self, device=None, budget_bytes: float = 120e9, max_batch: int = 256,
-                 max_batch_edges: float = 4e8, big_edges: int = 1 << 20):
+                 max_batch_edges: float = 4e8, big_edges: int = 1 << 20, threaded: bool = False):
         self.dev = core._device(device)
+        self.threaded = threaded  # builds on a worker thread (True) or on the serving loop
         self.big_edges = int(big_edges)
         self.budget = int(budget_bytes)
         self.max_batch = max_batch
@@ -305,7 +318,7 @@ class Server:
             for key, r, csr in job:
                 if csr is not None:
                     self._est[key] = sketch_bytes(r)
-            self._worker.inbox.put(job)
+            self._worker.submit(job)
         if taken:
             self.stats["ticks"] += 1
             self.stats["batch_sizes"].append(taken)
@@ -458,7 +471,8 @@ class Server:
         self._est: Dict[Tuple, int] = {}
         self.pending = []
         self._worker = _BuildWorker(self.dev, self.build_stream, self.big_edges)
-        self._worker.start()
+        if self.threaded:
+            self._worker.start()
         self._t0 = t0 = time.perf_counter()
         i = 0
         try:
@@ -477,8 +491,9 @@ class Server:
                     nxt = reqs[i].arrival - (time.perf_counter() - t0) if i < len(reqs) else 1.0
                     time.sleep(max(0.0, min(nxt, 0.0002)))
         finally:
-            self._worker.inbox.put(None)
-            self._worker.join(timeout=60)
+            if self.threaded:
+                self._worker.inbox.put(None)
+                self._worker.join(timeout=60)
         return sorted(self._done, key=lambda c: c.rid)
 
 
@@ -540,8 +555,8 @@ def _warm(dev) -> None:
     torch.cuda.synchronize(dev)
 
 
-def _compare(dev, reqs) -> Dict:
-    srv = Server(dev, budget_bytes=120e9)
+def _compare(dev, reqs, threaded: bool = False) -> Dict:
+    srv = Server(dev, budget_bytes=120e9, threaded=threaded)
     t0 = time.perf_counter()
     got = srv.serve(reqs)
     wall = time.perf_counter() - t0
@@ -574,6 +589,8 @@ def bench_entry(dev, quick: bool = True) -> Dict:
     _warm(dev)
     for rate in (50.0, 200.0, 1000.0):
         out[f"rate_{int(rate)}"] = _compare(dev, c5_requests(n, rate, seed=int(rate)))
+        if quick:  # the build worker thread instead of inline builds, for comparison
+            out[f"rate_{int(rate)}_threaded"] = _compare(dev, c5_requests(n, rate, seed=int(rate)), threaded=True)
     return out
 
 
