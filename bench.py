@@ -63,6 +63,9 @@ def parse_args():
                          "the saturating rate plus two lower rates, against the sequential path)")
     ap.add_argument("--p", type=int, default=12, help="HLL precision for --mode hybrid")
     ap.add_argument("--theta", type=int, default=HYB_THETA, help="sketch / route threshold for --mode hybrid")
+    ap.add_argument("--set", action="append", default=[], metavar="KEY=VALUE",
+                    help="launch-shape tuning for this run (core.set_count_tuning keys, e.g. bank_sort=1, hub=256); "
+                         "results do not depend on it")
     ap.add_argument("--replicas", action="store_true",
                     help="N>1: every rank counts its own copy of the graph (weak scaling) instead of the default "
                          "split of one graph's edges across the ranks (strong scaling)")
@@ -261,6 +264,9 @@ def run_ours(args):
         raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE={world}")
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if args.set:
+        core.set_count_tuning(**{**core.get_count_tuning(),
+                                 **{k: int(v) for k, v in (kv.split("=", 1) for kv in args.set)}})
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
