@@ -75,7 +75,7 @@ uint64_t tchll_launch_count(void);
  * rows and n_edges edges: the regrouped pair lists, per-vertex histograms and
  * offsets, the long-list work units, 16-byte-aligned copies of the probe
  * lists and, for hybrid counts, the HLL edge list -- about 20 bytes per edge
- * + 64 per vertex.  The aligned copies are optional: a workspace too small
+ * + 110 per vertex.  The aligned copies are optional: a workspace too small
  * for them but large enough otherwise runs without them (same results). */
 int tchll_count_workspace_bytes(int64_t n_nodes, int64_t n_edges, size_t* bytes);
 

@@ -94,6 +94,25 @@ def test_rmat_exact_vs_oracle(tchll, oracle, dev, scale):
     assert np.array_equal(_np(pe), pe_ref)
 
 
+def test_csr_sparse_ids_take_the_endpoint_sort_path(tchll, oracle, dev):
+    """Ids spread over [0, 2^30) (an odd multiplier mod 2^30 is one-to-one)
+    exceed twice the edge count, so the CSR build ranks endpoints by sorting
+    them instead of through the direct rank table; the CSR still equals the
+    oracle's and the count is that of the unspread graph."""
+    from triangle_counting_hll_b200 import core
+    import torch
+    u, v = core.gen_rmat(15, 16, 0.57, 0.19, 0.19, seed=4, device=dev)
+    spread = lambda t: ((t.to(torch.int64) * 2654435761) & ((1 << 30) - 1)).to(torch.int32)
+    su, sv = spread(u), spread(v)
+    assert int(torch.maximum(su, sv).max()) + 2 > 2 * su.numel()
+    g = core.csr_from_edges(su, sv)
+    og = _ocsr(oracle, _np(su), _np(sv))
+    _check_csr(g, og)
+    g0 = core.csr_from_edges(u, v)
+    assert _exact(core, g) == _exact(core, g0) == oracle.exact_count(og["row_ptr"], og["col_idx"], og["edge_u"],
+                                                                      og["edge_v"], nthreads=0)
+
+
 def test_rmat21_benched_configuration_exact_and_hybrid_vs_oracle(tchll, oracle, dev):
     """The benched configuration at scale 21 (R-MAT edge factor 16,
     (a,b,c) = (0.57,0.19,0.19), seed 1; 31.8 M oriented edges; scale 22 itself

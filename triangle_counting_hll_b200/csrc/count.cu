@@ -707,7 +707,7 @@ struct HubParams {
     const int32_t* pcol;  // padded lists in core coordinates (core_pad_kernel) or null: raw lists
     const int32_t* cidx;  // core index of each vertex, -1 outside the core (with pcol)
     const int32_t* n_core;  // device: core size C, vertex of core index kPlane (with pcol)
-    const int2* pl;         // packed lists: {plane-0 units, all units} per row
+    const int4* pl;         // packed lists per row: {first 16-byte unit, plane-0 units, all units, 0}
     int packed;             // packed 16-bit lists when C <= kCore16Max
     const HubSeg* segs;
     const unsigned long long* n_segs;
@@ -743,9 +743,11 @@ __device__ __forceinline__ int64_t pad_start(int32_t rs, int32_t y) {
 }
 
 // flag[w] = 1 for every w in N+(x) of every x with hub pairs: one warp per
-// hub segment (a segment names its x; an x with several segments is marked
-// more than once, idempotently).  Going by segments rather than by vertex id
-// keeps the warps balanced: hub vertices cluster at low ids in R-MAT graphs.
+// hub segment (a segment names its x; the segments of one x are consecutive,
+// and only the first marks x's list).  Going by segments rather than by
+// vertex id keeps the warps balanced: hub vertices cluster at low ids in
+// R-MAT graphs.  Each lane has four list members in flight (the loop is
+// bound by the latency of the dependent flag reads, not by bandwidth).
 // Values outside [0, n_nodes) are reported, not stored.
 __global__ void core_mark_kernel(const int32_t* __restrict__ row_ptr, int64_t n_nodes, int64_t nnz,
                                  const int32_t* __restrict__ col, const HubSeg* __restrict__ segs,
@@ -758,6 +760,7 @@ __global__ void core_mark_kernel(const int32_t* __restrict__ row_ptr, int64_t n_
     uint32_t status = 0;
     for (int64_t sg = warp; sg < nseg; sg += nwarps) {
         const int32_t x = segs[sg].x;
+        if (sg > 0 && segs[sg - 1].x == x) continue;  // x's first segment marks its list
         if (x < 0 || (int64_t)x >= n_nodes) {  // warp-uniform; cannot happen
             status |= ST_BAD_EDGE;
             continue;
@@ -767,16 +770,26 @@ __global__ void core_mark_kernel(const int32_t* __restrict__ row_ptr, int64_t n_
             status |= ST_BAD_ROW;
             continue;
         }
-        for (int32_t i = s + lane; i < e; i += 32) {
-            const int32_t w = __ldg(col + i);
+        for (int32_t i0 = s; i0 < e; i0 += 128) {
+            int32_t w[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int32_t i = i0 + 32 * k + lane;
+                w[k] = i < e ? __ldg(col + i) : -1;
+                if (i < e && (uint64_t)(uint32_t)w[k] >= (uint64_t)n_nodes) {
+                    status |= ST_BAD_KEY;
+                    w[k] = -1;
+                }
+            }
             // the core's members recur in many hub lists: read first, and
             // store only a flag not yet seen set (a stale 0 read just
             // repeats an idempotent store)
-            if ((uint64_t)(uint32_t)w < (uint64_t)n_nodes) {
-                if (flag[w] == 0) flag[w] = 1;
-            } else {
-                status |= ST_BAD_KEY;
-            }
+            int32_t f[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) f[k] = w[k] >= 0 ? flag[w[k]] : 1;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (f[k] == 0) flag[w[k]] = 1;
         }
     }
     status = __reduce_or_sync(FULL, status);
@@ -811,10 +824,12 @@ __global__ void core_index_kernel(int32_t* flag_cidx, const int32_t* __restrict_
 // 32-bit ones otherwise): row y starts at uint16 index pad16_start(y), a
 // multiple of 8 (16 bytes); plane 0 (members below the vertex of core index
 // kPlane) takes lo_units 16-byte units, plane 1 the next ones; pl[y] =
-// {lo_units, all units}.  roundup8(row_ptr[y]) + 24 y leaves room for both
-// planes' padding (at most 7 each) of every row before y.  Rows are sorted
-// (as every CSR of the reference is), so the planes split the row at one
-// position P, found by binary search; a member on the wrong side of P (an
+// {pad16_start(y) / 8, lo_units, all units, 0}, one 16-byte record so that
+// the hub kernel finds a pair's list with one load.  roundup8(row_ptr[y]) +
+// 24 y leaves room for both planes' padding (at most 7 each) of every row
+// before y.  Rows are sorted (as every CSR of the reference is), so the
+// planes split the row at one position P, found by an 8-way search down to
+// 64 members and a count of those; a member on the wrong side of P (an
 // unsorted row) or outside the core becomes padding and cannot match.
 __device__ __forceinline__ int64_t pad16_start(int32_t rs, int32_t y) {
     return (((int64_t)rs + 7) & ~(int64_t)7) + 24 * (int64_t)y;
@@ -844,7 +859,7 @@ __global__ void __launch_bounds__(256) core_pad16_kernel(const int32_t* __restri
                                                          const int32_t* __restrict__ cidx,
                                                          const int32_t* __restrict__ n_core, int packed,
                                                          int bank_sort, uint16_t* __restrict__ pcol16,
-                                                         int2* __restrict__ pl, tchll_count_result* result) {
+                                                         int4* __restrict__ pl, tchll_count_result* result) {
     __shared__ int s_cnt[32][32];  // per 8-lane group: bank counters, then cursors
     const int32_t C = n_core[0];
     if (!packed || C > kCore16Max) return;  // grid-uniform: the 32-bit lists apply
@@ -860,21 +875,31 @@ __global__ void __launch_bounds__(256) core_pad16_kernel(const int32_t* __restri
         const int32_t rs = __ldg(row_ptr + y), re = __ldg(row_ptr + y + 1);
         if (rs < 0 || re < rs || (int64_t)re > nnz) {
             status |= ST_BAD_ROW;
-            if (sub == 0) pl[y] = make_int2(0, 0);
+            if (sub == 0) pl[y] = make_int4(0, 0, 0, 0);
             continue;
         }
         const int32_t d = re - rs;
         int32_t P = d;
-        if (wsplit >= 0) {  // first member >= wsplit
+        if (wsplit >= 0) {  // P = first member >= wsplit, in [lo, hi]
             int32_t lo = 0, hi = d;
-            while (lo < hi) {
-                const int32_t mid = (lo + hi) >> 1;
-                if (__ldg(col + rs + mid) < wsplit) lo = mid + 1; else hi = mid;
+            while (hi - lo > 64) {  // group-uniform: 8 probes cut [lo, hi) into 9 parts
+                const int64_t len = hi - lo;
+                const bool lt = __ldg(col + rs + lo + (int32_t)(((sub + 1) * len) / 9)) < wsplit;
+                const int t = __popc((__ballot_sync(gmask, lt) >> (lane & 24)) & 0xFFu);
+                const int32_t nlo = t > 0 ? lo + (int32_t)((t * len) / 9) + 1 : lo;
+                hi = t < 8 ? lo + (int32_t)(((t + 1) * len) / 9) : hi;
+                lo = nlo;
             }
-            P = lo;
+            int c = 0;
+            for (int32_t m = lo + sub; m < hi; m += 8) c += __ldg(col + rs + m) < wsplit;
+            c += __shfl_xor_sync(gmask, c, 1);
+            c += __shfl_xor_sync(gmask, c, 2);
+            c += __shfl_xor_sync(gmask, c, 4);
+            P = lo + c;
         }
         const int32_t lo_units = (P + 7) >> 3, units = lo_units + ((d - P + 7) >> 3);
         const int64_t ps = pad16_start(rs, (int32_t)y);
+        const int4 rec = make_int4((int32_t)(ps >> 3), lo_units, units, 0);
         if (!bank_sort) {  // list order: one 16-byte unit per lane
             for (int32_t u = sub; u < units; u += 8) {
                 const int plane = u < lo_units ? 0 : 1;
@@ -887,13 +912,18 @@ __global__ void __launch_bounds__(256) core_pad16_kernel(const int32_t* __restri
                 *reinterpret_cast<uint4*>(pcol16 + ps + 8 * u) =
                     make_uint4(k[0] | (k[1] << 16), k[2] | (k[3] << 16), k[4] | (k[5] << 16), k[6] | (k[7] << 16));
             }
-            if (sub == 0) pl[y] = make_int2(lo_units, units);
+            if (sub == 0) pl[y] = rec;
             continue;
         }
         for (int plane = 0; plane < 2; ++plane) {
             const int32_t m0 = plane ? P : 0, m1 = plane ? d : P;
             if (m1 <= m0) continue;  // group-uniform
             uint16_t* out = pcol16 + ps + (plane ? 8 * (int64_t)lo_units : 0);
+            if (m1 - m0 <= 8) {  // one unit: one lane probes all its keys, order is moot
+                out[sub] = m0 + sub < m1 ? (uint16_t)plane_key(col, cidx, n_nodes, rs + m0 + sub, plane, status)
+                                         : (uint16_t)0xFFFFu;
+                continue;
+            }
             for (int b = sub; b < 32; b += 8) cnt[b] = 0;
             __syncwarp(gmask);
             for (int32_t m = m0 + sub; m < m1; m += 8)
@@ -922,7 +952,7 @@ __global__ void __launch_bounds__(256) core_pad16_kernel(const int32_t* __restri
             for (int32_t t = nk + sub; t < ((nk + 7) & ~7); t += 8) out[t] = 0xFFFFu;
             __syncwarp(gmask);  // the counters are reused by the next plane / row
         }
-        if (sub == 0) pl[y] = make_int2(lo_units, units);
+        if (sub == 0) pl[y] = rec;
     }
     status = __reduce_or_sync(FULL, status);
     if (lane == 0 && status) atomicOr(&result->status, status);
@@ -1405,20 +1435,18 @@ __global__ void __launch_bounds__(256, 8) hub_bitmap16_kernel(const HubParams H)
             r = __shfl_sync(FULL, r, 0);
             if (r >= sg.len) break;
             const int np = min(rsz, sg.len - r);
-            int32_t q0 = 0, nq = 0, lo = 0, rs = 0, re = 0;
+            int32_t y = 0, q0 = 0, nq = 0, lo = 0;
             if (lane < np) {
-                const int32_t y = __ldg(H.hy + sg.start + r + lane);
-                rs = __ldg(H.row_ptr + y);
-                re = __ldg(H.row_ptr + y + 1);
-                const int2 u = H.pl[y];
-                q0 = (int32_t)(pad16_start(rs, y) >> 3);
-                lo = u.x;
-                nq = u.y;
+                y = __ldg(H.hy + sg.start + r + lane);
+                const int4 u = H.pl[y];
+                q0 = u.x;
+                lo = u.y;
+                nq = u.z;
             }
             if (!table) {  // binary search per pair over the raw lists
                 for (int j = 0; j < np; ++j) {
-                    const int32_t jrs = __shfl_sync(FULL, rs, j);
-                    const int32_t jre = __shfl_sync(FULL, re, j);
+                    const int32_t yj = __shfl_sync(FULL, y, j);
+                    const int32_t jrs = __ldg(H.row_ptr + yj), jre = __ldg(H.row_ptr + yj + 1);
                     acc += warp_bsearch_count(col + xs, xl, col + jrs, jre - jrs, lane);
                 }
                 continue;
@@ -1706,7 +1734,10 @@ __device__ __forceinline__ double hll_estimate_from(U128 zsum, double extra, uin
 // the FP64 comparison) proves the estimator takes its linear-counting
 // branch: E = m * ln(m / V), the same expression the full estimator
 // evaluates, and Z is not needed.  Otherwise pass 2 forms Z exactly and
-// applies the full estimator.
+// applies the full estimator; the whole warp runs pass 2 for one such edge
+// at a time (coalesced loads, no lane idling while one group reads two
+// whole rows), so narrow groups cost nothing when a few of their edges need
+// the registers.
 // CACHE: each group takes a contiguous run of the edge list.  The routing
 // pass appends edges in CSR order, so consecutive HLL edges mostly share u,
 // and the group keeps u's zero mask in registers across them (up to four
@@ -1730,103 +1761,144 @@ __global__ void __launch_bounds__(256, CROW ? 2 : (CACHE ? 3 : 4)) hll_edges_ker
     const int64_t e_lo = CACHE ? gid * per : gid;
     const int64_t e_hi = CACHE ? min(n, e_lo + per) : n;
     const int64_t e_step = CACHE ? 1 : ngroups;
+    const int64_t w_first = gid - (lane / L);  // the warp's first group
     const int nq = H.zst >> 2;
     constexpr int KA = CROW ? 1 : 4;  // mask words cached per lane (p <= 10 with a cached row: one)
     const bool cache_a = CACHE && ZM && nq <= KA * L;
     int64_t cached = -1, cached_row = -1;
     uint4 ca[KA];
     uint4 ra[CROW ? 8 : 1];
-    for (int64_t e = e_lo; e < e_hi; e += e_step) {
-        const int32_t u = __ldg(H.hu + e), v = __ldg(H.hv + e);
-        const int64_t su = H.slot ? __ldg(H.slot + u) : (int64_t)u;
-        const int64_t sv = H.slot ? __ldg(H.slot + v) : (int64_t)v;
-        const uint4* a4 = reinterpret_cast<const uint4*>(H.regs + su * (int64_t)m);
-        const uint4* b4 = reinterpret_cast<const uint4*>(H.regs + sv * (int64_t)m);
-        double E;
+    // warp-uniform trip count (pass 2 is warp-wide): CACHE runs `per` steps,
+    // else while the warp's first group still has an edge
+    for (int64_t k = 0; CACHE ? k < per : w_first + k * ngroups < n; ++k) {
+        const int64_t e = e_lo + k * e_step;
+        const bool act = e < e_hi;  // group-uniform
+        int32_t u = 0, v = 0;
+        int64_t su = 0, sv = 0;
         uint32_t zeros = 0;
-        if (ZM) {  // registers zero in both rows: AND of the two zero masks
-            const uint4* za = reinterpret_cast<const uint4*>(H.zm + su * (int64_t)H.zst);
-            const uint4* zb = reinterpret_cast<const uint4*>(H.zm + sv * (int64_t)H.zst);
-            if (cache_a) {
-                if (su != cached) {  // group-uniform
+        if (act) {
+            u = __ldg(H.hu + e);
+            v = __ldg(H.hv + e);
+            su = H.slot ? __ldg(H.slot + u) : (int64_t)u;
+            sv = H.slot ? __ldg(H.slot + v) : (int64_t)v;
+            if (ZM) {  // registers zero in both rows: AND of the two zero masks
+                const uint4* za = reinterpret_cast<const uint4*>(H.zm + su * (int64_t)H.zst);
+                const uint4* zb = reinterpret_cast<const uint4*>(H.zm + sv * (int64_t)H.zst);
+                if (cache_a) {
+                    if (su != cached) {  // group-uniform
 #pragma unroll
-                    for (int k = 0; k < KA; ++k) {
-                        const int i = sub + k * L;
-                        ca[k] = i < nq ? __ldg(za + i) : make_uint4(0u, 0u, 0u, 0u);
+                        for (int kk = 0; kk < KA; ++kk) {
+                            const int i = sub + kk * L;
+                            ca[kk] = i < nq ? __ldg(za + i) : make_uint4(0u, 0u, 0u, 0u);
+                        }
+                        cached = su;
                     }
-                    cached = su;
-                }
 #pragma unroll
-                for (int k = 0; k < KA; ++k) {
-                    const int i = sub + k * L;
-                    if (i < nq) {
-                        const uint4 b = __ldg(zb + i);
-                        zeros += __popc(ca[k].x & b.x) + __popc(ca[k].y & b.y) + __popc(ca[k].z & b.z) +
-                                 __popc(ca[k].w & b.w);
+                    for (int kk = 0; kk < KA; ++kk) {
+                        const int i = sub + kk * L;
+                        if (i < nq) {
+                            const uint4 b = __ldg(zb + i);
+                            zeros += __popc(ca[kk].x & b.x) + __popc(ca[kk].y & b.y) + __popc(ca[kk].z & b.z) +
+                                     __popc(ca[kk].w & b.w);
+                        }
+                    }
+                } else {
+#pragma unroll 4
+                    for (int i = sub; i < nq; i += L) {
+                        const uint4 a = __ldg(za + i), b = __ldg(zb + i);
+                        zeros += __popc(a.x & b.x) + __popc(a.y & b.y) + __popc(a.z & b.z) + __popc(a.w & b.w);
                     }
                 }
             } else {
+                const uint4* a4 = reinterpret_cast<const uint4*>(H.regs + su * (int64_t)m);
+                const uint4* b4 = reinterpret_cast<const uint4*>(H.regs + sv * (int64_t)m);
 #pragma unroll 4
-                for (int i = sub; i < nq; i += L) {
-                    const uint4 a = __ldg(za + i), b = __ldg(zb + i);
-                    zeros += __popc(a.x & b.x) + __popc(a.y & b.y) + __popc(a.z & b.z) + __popc(a.w & b.w);
+                for (int i = sub; i < nvec; i += L) {
+                    const uint4 a = __ldg(a4 + i), b = __ldg(b4 + i);
+                    zeros += zero_bytes(a.x | b.x) + zero_bytes(a.y | b.y) + zero_bytes(a.z | b.z) +
+                             zero_bytes(a.w | b.w);
                 }
-            }
-        } else {
-#pragma unroll 4
-            for (int i = sub; i < nvec; i += L) {
-                const uint4 a = __ldg(a4 + i), b = __ldg(b4 + i);
-                zeros += zero_bytes(a.x | b.x) + zero_bytes(a.y | b.y) + zero_bytes(a.z | b.z) + zero_bytes(a.w | b.w);
             }
         }
         zeros = group_sum_u32<L>(zeros, gmask);
-        if (zeros >= H.lc_min) {
-            E = (double)m * log((double)m / (double)zeros);
-        } else {
-            uint32_t fast = 0, zz = 0;
-            uint64_t fine = 0;
-            double extra = 0.0;
-            if (CROW) {
+        const bool need = act && zeros < H.lc_min;  // group-uniform
+        double E = 0.0;
+        if (act && !need) E = (double)m * log((double)m / (double)zeros);
+        if (CROW) {
+            if (need) {  // the group forms Z itself, u's row kept in registers
+                uint32_t fast = 0, zz = 0;
+                uint64_t fine = 0;
+                double extra = 0.0;
+                const uint4* a4 = reinterpret_cast<const uint4*>(H.regs + su * (int64_t)m);
+                const uint4* b4 = reinterpret_cast<const uint4*>(H.regs + sv * (int64_t)m);
                 if (su != cached_row) {  // group-uniform
 #pragma unroll
-                    for (int k = 0; k < 8; ++k) {
-                        const int i = sub + k * L;
-                        ra[k] = i < nvec ? __ldg(a4 + i) : make_uint4(0u, 0u, 0u, 0u);
+                    for (int kk = 0; kk < 8; ++kk) {
+                        const int i = sub + kk * L;
+                        ra[kk] = i < nvec ? __ldg(a4 + i) : make_uint4(0u, 0u, 0u, 0u);
                     }
                     cached_row = su;
                 }
 #pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                    const int i = sub + k * L;
+                for (int kk = 0; kk < 8; ++kk) {
+                    const int i = sub + kk * L;
                     if (i < nvec) {
                         const uint4 b = __ldg(b4 + i);
-                        hll_word_lut(__vmaxu4(ra[k].x, b.x), S, fast, fine, zz, extra);
-                        hll_word_lut(__vmaxu4(ra[k].y, b.y), S, fast, fine, zz, extra);
-                        hll_word_lut(__vmaxu4(ra[k].z, b.z), S, fast, fine, zz, extra);
-                        hll_word_lut(__vmaxu4(ra[k].w, b.w), S, fast, fine, zz, extra);
+                        hll_word_lut(__vmaxu4(ra[kk].x, b.x), S, fast, fine, zz, extra);
+                        hll_word_lut(__vmaxu4(ra[kk].y, b.y), S, fast, fine, zz, extra);
+                        hll_word_lut(__vmaxu4(ra[kk].z, b.z), S, fast, fine, zz, extra);
+                        hll_word_lut(__vmaxu4(ra[kk].w, b.w), S, fast, fine, zz, extra);
                     }
                 }
-            } else {
+                fast = group_sum_u32<L>(fast, gmask);
+                fine = group_sum_u64<L>(fine, gmask);
+#pragma unroll
+                for (int o = L / 2; o > 0; o >>= 1) extra += __shfl_xor_sync(gmask, extra, o);
+                U128 z;  // fast * 2^(S-7) + fine; fast <= 2^(p+7)
+                z.lo = (uint64_t)fast << (S - 7);
+                z.hi = (uint64_t)fast >> (71 - S);
+                z.add(fine);
+                E = hll_estimate_from(z, extra, zeros, H.p, S, H.variant);
+            }
+        } else {
+            // pass 2, warp-wide: the whole warp forms Z for one edge at a
+            // time (coalesced 16-byte loads over both rows), for each group
+            // whose zero count left the linear-counting branch open
+            unsigned pend = __ballot_sync(FULL, need && sub == 0);
+            while (pend) {
+                const int f = __ffs(pend) - 1;  // the group's first lane
+                pend &= pend - 1;
+                const int64_t fsu = __shfl_sync(FULL, su, f), fsv = __shfl_sync(FULL, sv, f);
+                const uint32_t fz = __shfl_sync(FULL, zeros, f);
+                const uint4* a4 = reinterpret_cast<const uint4*>(H.regs + fsu * (int64_t)m);
+                const uint4* b4 = reinterpret_cast<const uint4*>(H.regs + fsv * (int64_t)m);
+                uint32_t fast = 0, zz = 0;
+                uint64_t fine = 0;
+                double extra = 0.0;
 #pragma unroll 2
-                for (int i = sub; i < nvec; i += L) {
+                for (int i = lane; i < nvec; i += 32) {
                     const uint4 a = __ldg(a4 + i), b = __ldg(b4 + i);
                     hll_word_lut(__vmaxu4(a.x, b.x), S, fast, fine, zz, extra);
                     hll_word_lut(__vmaxu4(a.y, b.y), S, fast, fine, zz, extra);
                     hll_word_lut(__vmaxu4(a.z, b.z), S, fast, fine, zz, extra);
                     hll_word_lut(__vmaxu4(a.w, b.w), S, fast, fine, zz, extra);
                 }
-            }
-            fast = group_sum_u32<L>(fast, gmask);
-            fine = group_sum_u64<L>(fine, gmask);
+                fast = group_sum_u32<32>(fast, FULL);
+                // registers of rank >= 8 (fine) and > S (extra, malformed rows) are rare
+                if (__any_sync(FULL, fine != 0)) fine = group_sum_u64<32>(fine, FULL);
+                if (__any_sync(FULL, extra != 0.0)) {
 #pragma unroll
-            for (int o = L / 2; o > 0; o >>= 1) extra += __shfl_xor_sync(gmask, extra, o);
-            U128 z;  // fast * 2^(S-7) + fine; fast <= 2^(p+7)
-            z.lo = (uint64_t)fast << (S - 7);
-            z.hi = (uint64_t)fast >> (71 - S);
-            z.add(fine);
-            E = hll_estimate_from(z, extra, zeros, H.p, S, H.variant);
+                    for (int o = 16; o > 0; o >>= 1) extra += __shfl_xor_sync(FULL, extra, o);
+                }
+                U128 z;  // fast * 2^(S-7) + fine; fast <= 2^(p+7)
+                z.lo = (uint64_t)fast << (S - 7);
+                z.hi = (uint64_t)fast >> (71 - S);
+                z.add(fine);
+                const double Ef = hll_estimate_from(z, extra, fz, H.p, S, H.variant);
+                if ((lane & ~(L - 1)) == f) E = Ef;
+            }
         }
-        if (sub == 0) {
+        if (act && sub == 0) {
             const int32_t du = __ldg(H.degrees + u), dv = __ldg(H.degrees + v);
             const double s_hat = (double)((int64_t)du + (int64_t)dv) - E;
             const double upper = (double)(du < dv ? du : dv);
@@ -1991,7 +2063,7 @@ struct CountWs {
     int32_t* cflag;           // n_nodes + 1: core flags, then core indices (with pcol)
     int32_t* cpos;            // n_nodes + 1: scan of the flags (with pcol)
     int32_t* ncore;           // core size, vertex of core index kPlane (with pcol)
-    int2* pl;                 // n_nodes: packed lists' {plane-0 units, all units} (with pcol)
+    int4* pl;                 // n_nodes: packed lists' {first unit, plane-0 units, all units, 0} (with pcol)
     void* tmp;
     size_t tmp_bytes;
 };
@@ -2028,7 +2100,7 @@ static bool carve_count(void* ws, size_t bytes, int64_t n_nodes, int64_t n_edges
     W.cflag = pad ? cv.take<int32_t>(N) : nullptr;
     W.cpos = pad ? cv.take<int32_t>(N) : nullptr;
     W.ncore = pad ? cv.take<int32_t>(4) : nullptr;
-    W.pl = pad ? cv.take<int2>(N) : nullptr;
+    W.pl = pad ? cv.take<int4>(N) : nullptr;
     W.tmp_bytes = tb;
     W.tmp = cv.take<char>(tb);
     if (need) *need = cv.off;

@@ -12,14 +12,22 @@
 //
 // Pipeline: largest id (one 16-byte read-back) -> pack canonical pairs into
 // 2k-bit keys, k = bits of the largest id -> radix sort -> unique -> node
-// table and remap -> degree histogram -> orient -> radix sort by (src, dst)
-// packed the same way -> scan.  The node table (compacted id = rank of the
-// raw id among the endpoints) comes from a direct table when the id space
-// fits the workspace (flag every endpoint id, scan the flags: rank[id] is the
-// scan, one gather per endpoint), else from sorting and deduplicating all
-// endpoints and a binary search per endpoint.  Sorting, unique and scans use
-// CUB (header templates compiled into this library); the other passes are
-// kernels written here.
+// table and remap -> degree histogram -> orient -> stable radix sort of the
+// (src, dst) pairs by src alone -> row pointers from the sorted sources.
+// The node table (compacted id = rank of the raw id among the endpoints)
+// comes from a direct table when the id space fits the workspace (flag every
+// endpoint id, scan the flags: rank[id] is the scan, one gather per
+// endpoint), else from sorting and deduplicating all endpoints and a binary
+// search per endpoint.
+//
+// One sort by src is enough for rows sorted by dst: the pairs reach it in
+// canonical (a, b) order, a < b, and compaction keeps that order.  For a
+// source s, the edges it gained by flipping (b = s, dst a < s) come before
+// the edges it kept (a = s, dst b > s), each group in ascending dst, so a
+// stable sort by src leaves every row ascending.
+//
+// Sorting, unique and scans use CUB (header templates compiled into this
+// library); the other passes are kernels written here.
 #include <cub/cub.cuh>
 
 #include "common.cuh"
@@ -48,17 +56,20 @@ struct CsrWs {
 
 static size_t csr_cub_tmp(int64_t n_raw) {
     const int R = (int)(n_raw > 0 ? n_raw : 1);
-    size_t a = 0, b = 0, c = 0, d = 0, e = 0;
+    size_t a = 0, b = 0, c = 0, d = 0, e = 0, f = 0;
     cub::DeviceRadixSort::SortKeys(nullptr, a, (uint64_t*)nullptr, (uint64_t*)nullptr, R, 0, 63);
     cub::DeviceSelect::Unique(nullptr, b, (uint64_t*)nullptr, (uint64_t*)nullptr, (int64_t*)nullptr, R);
     cub::DeviceRadixSort::SortKeys(nullptr, c, (uint32_t*)nullptr, (uint32_t*)nullptr, 2 * R, 0, 32);
     cub::DeviceSelect::Unique(nullptr, d, (uint32_t*)nullptr, (uint32_t*)nullptr, (int64_t*)nullptr, 2 * R);
     cub::DeviceScan::ExclusiveSum(nullptr, e, (int32_t*)nullptr, (int32_t*)nullptr, 2 * R + 1);
+    cub::DeviceRadixSort::SortPairs(nullptr, f, (uint32_t*)nullptr, (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                    (uint32_t*)nullptr, R, 0, 32);
     size_t m = a;
     if (b > m) m = b;
     if (c > m) m = c;
     if (d > m) m = d;
     if (e > m) m = e;
+    if (f > m) m = f;
     return m;
 }
 
@@ -89,6 +100,13 @@ static int grid_n(int64_t n, int threads = 256) {
 
 #define GRID_STRIDE(i, n) \
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
+
+// Grid-stride loop that whole warps enter and leave together (bodies with
+// warp shuffles): i may reach past n in the last pass; test it in the body.
+#define WARP_GRID_STRIDE(i, n)                                                               \
+    for (int64_t _wb = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31u),              \
+                 i = _wb + (threadIdx.x & 31u);                                              \
+         _wb < (n); _wb += (int64_t)gridDim.x * blockDim.x, i = _wb + (threadIdx.x & 31u))
 
 // Largest endpoint id (atomicMax, one per warp) and the negative-id flag.
 __global__ void max_id_kernel(const int32_t* __restrict__ ru, const int32_t* __restrict__ rv, int64_t n,
@@ -154,35 +172,62 @@ __device__ __forceinline__ int64_t n_real_nodes(const uint32_t* nodes, const int
     return (nn > 0 && nodes[nn - 1] == kEndSentinel) ? nn - 1 : nn;
 }
 
+// deg[a] += (number of lanes with this a) from the last lane of each run of
+// equal a (the keys are sorted by a, so runs are contiguous lanes); lanes
+// past the end pass a = -1.
+__device__ __forceinline__ void add_runs(int32_t* deg, int32_t a, int lane) {
+    const unsigned FULLM = 0xFFFFFFFFu;
+    const int32_t na = __shfl_down_sync(FULLM, a, 1);
+    const bool tail = lane == 31 || na != a;  // the run's last lane
+    const unsigned tails = __ballot_sync(FULLM, tail);
+    if (a >= 0 && tail) {
+        // the run starts after the previous tail
+        const unsigned below = tails & ((1u << lane) - 1u);
+        const int start = below ? 32 - __clz(below) : 0;
+        atomicAdd(deg + a, lane - start + 1);
+    }
+}
+
 // Sort path: binary search of both endpoints in the sorted node table.
 __global__ void remap_kernel(const uint64_t* __restrict__ keys, int64_t cap, const uint32_t* __restrict__ nodes,
                              const int64_t* cnt, int kb, int32_t* ca, int32_t* cb, int32_t* deg) {
     const int64_t ne = n_real_edges(keys, cnt, kb);
     const int64_t nn = n_real_nodes(nodes, cnt);
     const uint64_t lo = (1ull << kb) - 1ull;
-    GRID_STRIDE(i, cap) {
-        if (i >= ne) break;
-        const uint64_t k = keys[i];
-        const int32_t a = (int32_t)lower_bound_u32(nodes, nn, (uint32_t)(k >> kb));
-        const int32_t b = (int32_t)lower_bound_u32(nodes, nn, (uint32_t)(k & lo));
-        ca[i] = a;
-        cb[i] = b;
-        atomicAdd(deg + a, 1);
-        atomicAdd(deg + b, 1);
+    const int lane = threadIdx.x & 31;
+    WARP_GRID_STRIDE(i, cap) {
+        const bool in = i < ne;
+        int32_t a = -1;
+        if (in) {
+            const uint64_t k = keys[i];
+            a = (int32_t)lower_bound_u32(nodes, nn, (uint32_t)(k >> kb));
+            const int32_t b = (int32_t)lower_bound_u32(nodes, nn, (uint32_t)(k & lo));
+            ca[i] = a;
+            cb[i] = b;
+            atomicAdd(deg + b, 1);
+        }
+        add_runs(deg, a, lane);
     }
 }
 
 // Direct path: flag[id] = 1 for both endpoints of every unique edge (flag
-// zeroed over [0, max id + 1] before).
+// zeroed over [0, max id + 1] before).  The keys are sorted, so neighbouring
+// lanes mostly share a: only the first lane of each run stores it.
 __global__ void flag_ends_kernel(const uint64_t* __restrict__ keys, int64_t cap, const int64_t* cnt, int kb,
                                  int32_t* flag) {
     const int64_t ne = n_real_edges(keys, cnt, kb);
     const uint64_t lo = (1ull << kb) - 1ull;
-    GRID_STRIDE(i, cap) {
-        if (i >= ne) break;
-        const uint64_t k = keys[i];
-        flag[k >> kb] = 1;
-        flag[k & lo] = 1;
+    const int lane = threadIdx.x & 31;
+    WARP_GRID_STRIDE(i, cap) {
+        const bool in = i < ne;
+        const uint64_t k = in ? keys[i] : 0;
+        const uint32_t a = (uint32_t)(k >> kb);
+        const uint32_t pa = __shfl_up_sync(0xFFFFFFFFu, a, 1);
+        const bool pin = __shfl_up_sync(0xFFFFFFFFu, (int)in, 1) != 0;
+        if (in) {
+            if (lane == 0 || !pin || pa != a) flag[a] = 1;
+            flag[k & lo] = 1;
+        }
     }
 }
 
@@ -202,14 +247,19 @@ __global__ void remap_direct_kernel(const uint64_t* __restrict__ keys, int64_t c
                                     const int64_t* cnt, int kb, int32_t* ca, int32_t* cb, int32_t* deg) {
     const int64_t ne = n_real_edges(keys, cnt, kb);
     const uint64_t lo = (1ull << kb) - 1ull;
-    GRID_STRIDE(i, cap) {
-        if (i >= ne) break;
-        const uint64_t k = keys[i];
-        const int32_t a = __ldg(rank + (k >> kb)), b = __ldg(rank + (k & lo));
-        ca[i] = a;
-        cb[i] = b;
-        atomicAdd(deg + a, 1);
-        atomicAdd(deg + b, 1);
+    const int lane = threadIdx.x & 31;
+    WARP_GRID_STRIDE(i, cap) {
+        const bool in = i < ne;
+        int32_t a = -1;
+        if (in) {
+            const uint64_t k = keys[i];
+            a = __ldg(rank + (k >> kb));
+            const int32_t b = __ldg(rank + (k & lo));
+            ca[i] = a;
+            cb[i] = b;
+            atomicAdd(deg + b, 1);
+        }
+        add_runs(deg, a, lane);
     }
 }
 
@@ -224,38 +274,36 @@ __global__ void sizes_kernel(const uint64_t* keys, const uint32_t* nodes, const 
     sizes[1] = n_real_edges(keys, cnt, kb);
 }
 
-// Orientation u -> v iff (deg u, u) < (deg v, v); oriented keys (s << kn) | d
-// with kn = bits of the largest compacted id.
+// Orientation u -> v iff (deg u, u) < (deg v, v): the pair (src, dst) of
+// edge i goes to okey[i] / oval[i] (canonical order kept for the stable sort).
 __global__ void orient_kernel(const int32_t* __restrict__ ca, const int32_t* __restrict__ cb, int64_t ne,
-                              const int32_t* __restrict__ deg, int kn, int32_t* fdeg, uint64_t* okeys) {
+                              const int32_t* __restrict__ deg, uint32_t* okey, uint32_t* oval) {
     GRID_STRIDE(i, ne) {
         const int32_t a = ca[i], b = cb[i];
         const int32_t da = deg[a], db = deg[b];
         const bool first = (da < db) || (da == db && a < b);
-        const int32_t s = first ? a : b, d = first ? b : a;
-        atomicAdd(fdeg + s, 1);
-        okeys[i] = ((uint64_t)(uint32_t)s << kn) | (uint32_t)d;
+        okey[i] = (uint32_t)(first ? a : b);
+        oval[i] = (uint32_t)(first ? b : a);
     }
 }
 
-__global__ void split_kernel(const uint64_t* __restrict__ okeys, int64_t ne, int kn, int32_t* col_idx,
-                             int32_t* edge_u, int32_t* edge_v) {
-    const uint64_t lo = (1ull << kn) - 1ull;
-    GRID_STRIDE(i, ne) {
-        const uint64_t k = okeys[i];
-        const int32_t d = (int32_t)(k & lo);
-        edge_u[i] = (int32_t)(k >> kn);
-        col_idx[i] = d;
-        edge_v[i] = d;
+// row_ptr from the ascending sources src[0 .. ne): entry i is the first edge
+// of every row s in (src[i-1], src[i]] (src[-1] = -1, src[ne] = n_nodes),
+// so each of row_ptr[0 .. n_nodes] is written exactly once.
+__global__ void row_ptr_kernel(const int32_t* __restrict__ src, int64_t ne, int64_t n_nodes, int32_t* row_ptr) {
+    GRID_STRIDE(i, ne + 1) {
+        const int64_t lo = i > 0 ? (int64_t)src[i - 1] : -1;
+        const int64_t hi = i < ne ? (int64_t)src[i] : n_nodes;
+        for (int64_t r = lo + 1; r <= hi; ++r) row_ptr[r] = (int32_t)i;
     }
 }
 
-__global__ void copy_nodes_kernel(const uint32_t* __restrict__ nodes, int64_t n, const int32_t* __restrict__ fdeg,
+__global__ void copy_nodes_kernel(const uint32_t* __restrict__ nodes, int64_t n, const int32_t* __restrict__ row_ptr,
                                   const int32_t* __restrict__ deg, int32_t* node_ids, int32_t* degrees,
                                   int32_t* undirected) {
     GRID_STRIDE(i, n) {
         node_ids[i] = (int32_t)nodes[i];
-        degrees[i] = fdeg[i];
+        degrees[i] = row_ptr[i + 1] - row_ptr[i];
         if (undirected) undirected[i] = deg[i];
     }
 }
@@ -419,22 +467,24 @@ TCHLL_EXPORT int tchll_csr_build_phase2(int64_t n_raw, int64_t n_nodes, int64_t 
         return TCHLL_EWORKSPACE;
     }
     cudaStream_t st = (cudaStream_t)stream;
-    TCHLL_CUDA(cudaMemsetAsync(W.fdeg, 0, ((size_t)n_nodes + 1) * sizeof(int32_t), st));
     if (n_edges > 0) {
+        // the pairs in the first half of k1's bytes (2 n_raw uint32 >= 2 n_edges);
+        // sorted by src straight into edge_u (src) and col_idx (dst)
+        uint32_t* okey = reinterpret_cast<uint32_t*>(W.k1);
+        uint32_t* oval = okey + n_edges;
         const int kn = bits_for(n_nodes > 1 ? n_nodes - 1 : 1);
-        orient_kernel<<<grid_n(n_edges), 256, 0, st>>>(W.ca, W.cb, n_edges, W.deg, kn, W.fdeg, W.k1);
+        orient_kernel<<<grid_n(n_edges), 256, 0, st>>>(W.ca, W.cb, n_edges, W.deg, okey, oval);
         TCHLL_CHECK_LAUNCH("orient_kernel");
         size_t tb = W.tmp_bytes;
-        TCHLL_CUDA(cub::DeviceRadixSort::SortKeys(W.tmp, tb, W.k1, W.k0, (int)n_edges, 0, 2 * kn, st));
+        TCHLL_CUDA(cub::DeviceRadixSort::SortPairs(W.tmp, tb, okey, reinterpret_cast<uint32_t*>(edge_u), oval,
+                                                   reinterpret_cast<uint32_t*>(col_idx), (int)n_edges, 0, kn, st));
         count_launch();
-        split_kernel<<<grid_n(n_edges), 256, 0, st>>>(W.k0, n_edges, kn, col_idx, edge_u, edge_v);
-        TCHLL_CHECK_LAUNCH("split_kernel");
+        TCHLL_CUDA(cudaMemcpyAsync(edge_v, col_idx, (size_t)n_edges * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
     }
-    size_t tb = W.tmp_bytes;
-    TCHLL_CUDA(cub::DeviceScan::ExclusiveSum(W.tmp, tb, W.fdeg, row_ptr, (int)(n_nodes + 1), st));
-    count_launch();
+    row_ptr_kernel<<<grid_n(n_edges + 1), 256, 0, st>>>(edge_u, n_edges, n_nodes, row_ptr);
+    TCHLL_CHECK_LAUNCH("row_ptr_kernel");
     if (n_nodes > 0) {
-        copy_nodes_kernel<<<grid_n(n_nodes), 256, 0, st>>>(W.e0, n_nodes, W.fdeg, W.deg, node_ids, degrees,
+        copy_nodes_kernel<<<grid_n(n_nodes), 256, 0, st>>>(W.e0, n_nodes, row_ptr, W.deg, node_ids, degrees,
                                                             undirected_degrees);
         TCHLL_CHECK_LAUNCH("copy_nodes_kernel");
     }

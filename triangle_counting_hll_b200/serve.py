@@ -225,9 +225,9 @@ class Server:
     docstring."""
 
     def __init__(self, device=None, budget_bytes: float = 120e9, max_batch: int = 256,
-                 max_batch_edges: float = 4e8, big_edges: int = 1 << 20, threaded: bool = False):
+                 max_batch_edges: float = 4e8, big_edges: int = 1 << 20, threaded: bool = True):
         self.dev = core._device(device)
-        self.threaded = threaded  # builds on a worker thread (True) or on the serving loop
+        self.threaded = threaded  # builds on a worker thread (True) or on the serving loop (False)
         self.big_edges = int(big_edges)
         self.budget = int(budget_bytes)
         self.max_batch = max_batch
@@ -555,7 +555,7 @@ def _warm(dev) -> None:
     torch.cuda.synchronize(dev)
 
 
-def _compare(dev, reqs, threaded: bool = False) -> Dict:
+def _compare(dev, reqs, threaded: bool = True) -> Dict:
     srv = Server(dev, budget_bytes=120e9, threaded=threaded)
     t0 = time.perf_counter()
     got = srv.serve(reqs)
@@ -589,8 +589,8 @@ def bench_entry(dev, quick: bool = True) -> Dict:
     _warm(dev)
     for rate in (50.0, 200.0, 1000.0):
         out[f"rate_{int(rate)}"] = _compare(dev, c5_requests(n, rate, seed=int(rate)))
-        if quick:  # the build worker thread instead of inline builds, for comparison
-            out[f"rate_{int(rate)}_threaded"] = _compare(dev, c5_requests(n, rate, seed=int(rate)), threaded=True)
+        if quick:  # builds on the serving loop instead of the worker thread, for comparison
+            out[f"rate_{int(rate)}_inline"] = _compare(dev, c5_requests(n, rate, seed=int(rate)), threaded=False)
     return out
 
 
