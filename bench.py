@@ -635,10 +635,20 @@ def hybrid_sweep(g, exact_count: int, dev, exact_ms: float = None) -> dict:
             ms = s.elapsed_time(e)
             best = ms if best is None else min(best, ms)
         total, r = core.hybrid_from_result(res)
+        # one more call with phase events: the HLL pass (zero masks + edge
+        # estimates, on the second stream) and the exact-routed part
+        core.set_phase_timing(True)
+        core.hybrid_count_compact_tensors(g.row_ptr, g.col_idx, g.edge_u, g.edge_v, g.degrees, rows, slot, p,
+                                          theta, split_kernels=True, result=res)
+        torch.cuda.synchronize()
+        ph = core.phase_times()
+        core.set_phase_timing(False)
         out[key] = {"theta": theta, "gamma": theta, "p": p, "ms": best, "edges_per_s": g.n_edges / (best / 1e3),
                     "sketch_build_ms": build_ms, "n_sketched": n_rows, "estimate": total,
                     "rel_err": abs(total - exact_count) / exact_count, "n_approx": int(r.n_approx),
-                    "clamp_ratio": int(r.n_clamped) / max(int(r.n_approx), 1)}
+                    "clamp_ratio": int(r.n_clamped) / max(int(r.n_approx), 1),
+                    "hll_pass_ms": ph.get("hll"),
+                    "exact_part_ms": (ph.get("pairs") or 0.0) + (ph.get("count") or 0.0)}
         if exact_ms:
             out[key]["speedup_vs_exact"] = exact_ms / best
         del rows, slot

@@ -101,6 +101,17 @@ int tchll_exact_count(const int32_t* row_ptr, int64_t n_nodes, const int32_t* co
                       int64_t* per_edge_support, tchll_count_result* result, void* workspace,
                       size_t workspace_bytes, void* stream);
 
+/* tchll_exact_count (no per-edge output) for a col_idx still being copied:
+ * the kernels that read col_idx first wait for col_ready_event (a
+ * cudaEvent_t recorded after the copy that fills col_idx; NULL: ready), so
+ * the pair regrouping, which reads only row_ptr and the edges, overlaps that
+ * copy.  row_ptr, edge_u and edge_v must be ready in stream order.  Same
+ * result as tchll_exact_count. */
+int tchll_exact_count_staged(const int32_t* row_ptr, int64_t n_nodes, const int32_t* col_idx, int64_t nnz,
+                             const int32_t* edge_u, const int32_t* edge_v, int64_t n_edges,
+                             tchll_count_result* result, void* workspace, size_t workspace_bytes,
+                             void* col_ready_event, void* stream);
+
 /*
  * Hybrid count over DENSE sketches (row v at sketch_regs + v * 2^p, present
  * iff has_sketch[v] == 1).  An edge goes to HLL iff

@@ -173,6 +173,24 @@ def _foreign_to_device():
     return _CAIArray, "cuda_array_interface"
 
 
+def test_host_arrays_staged_copies(tchll, oracle, dev):
+    """gpu_exact_triangle_count on host arrays (pinned torch tensors, plain
+    numpy) copies them in stages beside the count (the regrouping runs while
+    col_idx is still in flight); the count equals the oracle's, and a
+    following device-array call on the same stream sees the same."""
+    from triangle_counting_hll_b200 import core
+    u, v = core.gen_rmat(16, 16, 0.57, 0.19, 0.19, seed=8, device=dev)
+    g = core.csr_from_edges(u, v)
+    og = _ocsr(oracle, _np(u), _np(v))
+    want = oracle.exact_count(og["row_ptr"], og["col_idx"], og["edge_u"], og["edge_v"])
+    pinned = [t.cpu().pin_memory() for t in (g.row_ptr, g.col_idx, g.edge_u, g.edge_v)]
+    for _ in range(3):
+        assert tchll.gpu_exact_triangle_count(*pinned)[0] == want
+    plain = [og[k] for k in ("row_ptr", "col_idx", "edge_u", "edge_v")]
+    assert tchll.gpu_exact_triangle_count(*plain)[0] == want
+    assert tchll.gpu_exact_triangle_count(g.row_ptr, g.col_idx, g.edge_u, g.edge_v)[0] == want
+
+
 def test_numba_device_arrays_at_the_reference_entry_points(tchll, oracle, dev):
     """The reference's driver hands Numba device arrays (cuda.to_device of
     the CSR, experiment/exp_gpu.py:686-692) to gpu_exact_triangle_count,

@@ -62,6 +62,7 @@ SIGNATURES = {
     "tchll_count_workspace_bytes": (C.c_int, [_I64, _I64, C.POINTER(_SZ)]),
     "tchll_hybrid_workspace_bytes": (C.c_int, [_I64, _I64, _I64, C.c_int32, C.POINTER(_SZ)]),
     "tchll_exact_count": (C.c_int, [_P, _I64, _P, _I64, _P, _P, _I64, _P, _P, _P, _SZ, _P]),
+    "tchll_exact_count_staged": (C.c_int, [_P, _I64, _P, _I64, _P, _P, _I64, _P, _P, _SZ, _P, _P]),
     "tchll_hybrid_count_dense": (C.c_int, [_P, _I64, _P, _I64, _P, _P, _I64, _P, _P, _P, _I32, _I64, _I32,
                                            _P, _P, _SZ, _P]),
     "tchll_hybrid_count_compact": (C.c_int, [_P, _I64, _P, _I64, _P, _P, _I64, _P, _P, _I64, _P, _I32, _I64,

@@ -8,7 +8,7 @@ from __future__ import annotations
 import ctypes as C
 import math
 from dataclasses import dataclass
-from typing import Optional, Tuple
+from typing import Dict, Optional, Tuple
 
 import numpy as np
 import torch
@@ -198,6 +198,53 @@ def exact_count_tensors(row_ptr: torch.Tensor, col_idx: torch.Tensor, edge_u: to
                                    ptr(edge_v), n_edges, ptr(pe), ptr(res), ptr(ws), ws.numel(),
                                    stream_handle(dev)), "exact count")
     return res, pe
+
+
+_COPY_STREAMS: Dict[int, torch.cuda.Stream] = {}
+
+
+def _copy_stream(dev: torch.device) -> torch.cuda.Stream:
+    i = dev.index if dev.index is not None else torch.cuda.current_device()
+    if i not in _COPY_STREAMS:
+        _COPY_STREAMS[i] = torch.cuda.Stream(device=i)
+    return _COPY_STREAMS[i]
+
+
+def exact_count_host(row_ptr: torch.Tensor, col_idx: torch.Tensor, edge_u: torch.Tensor, edge_v: torch.Tensor,
+                     device=None, result: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """Exact count of a CSR held in host memory (pinned for asynchronous
+    copies).  The arrays are copied on a copy stream in the order row_ptr,
+    edge_u, edge_v, col_idx, and the count (tchll_exact_count_staged) starts
+    once the first three have arrived: the pair regrouping, which reads only
+    those, runs while col_idx is still crossing the host link.  Returns the
+    device result block; stream-ordered on the current stream."""
+    dev = _device(device)
+    cs = _copy_stream(dev)
+    cur = torch.cuda.current_stream(dev)
+    cs.wait_stream(cur)  # the copies may overwrite nothing the caller still uses
+    with torch.cuda.stream(cs):
+        d = [t.to(device=dev, dtype=torch.int32, non_blocking=True).contiguous()
+             for t in (row_ptr, edge_u, edge_v)]
+        head = torch.cuda.Event()
+        head.record(cs)
+        ci = col_idx.to(device=dev, dtype=torch.int32, non_blocking=True).contiguous()
+        col_ready = torch.cuda.Event()
+        col_ready.record(cs)
+    for t in (*d, ci):  # allocated on the copy stream, used on the current one
+        t.record_stream(cur)
+    cur.wait_event(head)
+    rp, eu, ev = d
+    n_nodes = int(rp.numel()) - 1
+    n_edges = int(eu.numel())
+    if int(ev.numel()) != n_edges:
+        raise ValueError("edge_u and edge_v differ in length")
+    res = result if result is not None else _lib.count_result_tensor(dev)
+    ws = _count_ws(n_nodes, n_edges, dev)
+    check(load().tchll_exact_count_staged(ptr(rp), n_nodes, ptr(ci), int(ci.numel()), ptr(eu), ptr(ev), n_edges,
+                                          ptr(res), ptr(ws), ws.numel(), col_ready.cuda_event,
+                                          stream_handle(dev)), "exact count")
+    cur.wait_event(col_ready)  # col_idx is in use until the count ends
+    return res
 
 
 def hybrid_count_dense_tensors(row_ptr, col_idx, edge_u, edge_v, degrees, sketch_regs, has_sketch, gamma: int,

@@ -160,8 +160,10 @@ __device__ __forceinline__ int ceil_log2_i(int x) { return x <= 1 ? 0 : 32 - __c
 // Loads and validates edge e; returns false (and flags status) when malformed.
 __device__ __forceinline__ bool load_edge(const CountParams& P, int64_t e, int32_t& u, int32_t& v, int32_t& us,
                                           int32_t& ue, int32_t& vs, int32_t& ve, uint32_t& status) {
-    u = __ldg(P.edge_u + e);
-    v = __ldg(P.edge_v + e);
+    // the edge arrays stream through once per pass: evict-first loads keep
+    // L1 for the row_ptr entries of the high-degree endpoints, which recur
+    u = __ldcs(P.edge_u + e);
+    v = __ldcs(P.edge_v + e);
     if (u < 0 || v < 0 || (int64_t)u >= P.n_nodes || (int64_t)v >= P.n_nodes) {
         status |= ST_BAD_EDGE;
         return false;
@@ -232,15 +234,34 @@ __device__ __forceinline__ int64_t graph_of(const int32_t* vbase, int64_t n_grap
     return lo;
 }
 
+// Lanes whose pairs share x in a run of consecutive lanes (edges in CSR
+// order share u, so the pairs with x = u come in runs): the run's first lane
+// (head) and its length.  key must differ between lanes that may not merge.
+// Whole warps call it (the grid-stride loops below are warp-uniform).
+__device__ __forceinline__ void lane_runs(int32_t key, int lane, int& head_lane, int& run_len) {
+    const int32_t prev = __shfl_up_sync(FULL, key, 1);
+    const unsigned heads = __ballot_sync(FULL, lane == 0 || prev != key);
+    const unsigned le = (2u << lane) - 1u;
+    head_lane = 31 - __clz(heads & le);
+    const unsigned after = heads & ~((2u << head_lane) - 1u);  // heads after this run's head
+    run_len = (after ? __ffs(after) - 1 : 32) - head_lane;
+}
+
+// Grid-stride loop that whole warps enter and leave together: e may reach
+// past n in the last pass; the body tests it.
+#define WARP_EDGE_LOOP(e, n)                                                                   \
+    for (int64_t _wb = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31u),                \
+                 e = _wb + (threadIdx.x & 31u);                                                \
+         _wb < (n); _wb += (int64_t)gridDim.x * blockDim.x, e = _wb + (threadIdx.x & 31u))
+
 template <bool HYB>
 __global__ void pair_hist_kernel(const CountParams P, int32_t* cnt) {
     uint32_t status = 0;
     unsigned long long fallback = 0;
     const int lane = threadIdx.x & 31;
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < P.n_edges;
-         e += (int64_t)gridDim.x * blockDim.x) {
-        int32_t u, v, us, ue, vs, ve;
-        bool ok = load_edge(P, e, u, v, us, ue, vs, ve, status);
+    WARP_EDGE_LOOP(e, P.n_edges) {
+        int32_t u = 0, v = 0, us = 0, ue = 0, vs = 0, ve = 0;
+        bool ok = e < P.n_edges && load_edge(P, e, u, v, us, ue, vs, ve, status);
         bool hll = false;
         if (HYB && ok) {
             int32_t du, dv;
@@ -256,21 +277,20 @@ __global__ void pair_hist_kernel(const CountParams P, int32_t* cnt) {
             }
         }
         {
-            // lanes with the same table side (consecutive CSR edges share u)
-            // add with one atomic
-            const int32_t x = (ok && !hll) ? (((ue - us) >= (ve - vs)) ? u : v) : -1;
-            const unsigned peers = __match_any_sync(__activemask(), x);
-            if (x >= 0 && lane == __ffs(peers) - 1) atomicAdd(cnt + x, __popc(peers));
+            // a run of lanes with the same table side adds with one atomic
+            const bool counted = ok && !hll;
+            const int32_t x = counted ? (((ue - us) >= (ve - vs)) ? u : v) : -1 - lane;
+            int head, len;
+            lane_runs(x, lane, head, len);
+            if (counted && lane == head) atomicAdd(cnt + x, len);
         }
         if (HYB && P.hll_u) {
             // warp-aggregated append of the HLL-routed edges
-            const unsigned act = __activemask();
-            const unsigned bal = __ballot_sync(act, hll);
+            const unsigned bal = __ballot_sync(FULL, hll);
             if (bal) {
-                const int leader = __ffs(act) - 1;
                 unsigned long long base = 0;
-                if (lane == leader) base = atomicAdd(P.hll_n, (unsigned long long)__popc(bal));
-                base = __shfl_sync(act, base, leader);
+                if (lane == 0) base = atomicAdd(P.hll_n, (unsigned long long)__popc(bal));
+                base = __shfl_sync(FULL, base, 0);
                 if (hll) {
                     const unsigned long long pos = base + __popc(bal & ((1u << lane) - 1u));
                     P.hll_u[pos] = u;
@@ -291,20 +311,19 @@ __global__ void pair_scatter_kernel(const CountParams P, int32_t* cursor, int32_
     uint32_t status = 0;
     const int lane = threadIdx.x & 31;
     const int64_t hbase = hub > 0 ? (int64_t)*n_small : 0;
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < P.n_edges;
-         e += (int64_t)gridDim.x * blockDim.x) {
+    WARP_EDGE_LOOP(e, P.n_edges) {
         int32_t x = 0, y = 0, xl = 0;
-        const bool ok = pair_of<HYB>(P, e, x, y, xl, status);
-        // lanes with the same x claim their positions with one atomic (x's
-        // list length, hence its list, is the same for all of them)
-        const unsigned peers = __match_any_sync(__activemask(), ok ? x : -1);
+        const bool ok = e < P.n_edges && pair_of<HYB>(P, e, x, y, xl, status);
+        // a run of lanes with the same x claims its positions with one
+        // atomic (x's list length, hence its list, is the same for all)
+        int head, len;
+        lane_runs(ok ? x : -1 - lane, lane, head, len);
+        const bool to_hub = hub > 0 && xl > hub;
+        int32_t base = 0;
+        if (ok && lane == head) base = atomicAdd((to_hub ? cursorh : cursor) + x, len);
+        base = __shfl_sync(FULL, base, head);
         if (ok) {
-            const int leader = __ffs(peers) - 1;
-            const bool to_hub = hub > 0 && xl > hub;
-            int32_t base = 0;
-            if (lane == leader) base = atomicAdd((to_hub ? cursorh : cursor) + x, __popc(peers));
-            base = __shfl_sync(peers, base, leader);
-            const int32_t pos = base + __popc(peers & ((1u << lane) - 1u));
+            const int32_t pos = base + (lane - head);
             if (to_hub) {
                 py[hbase + pos] = y;
             } else {
@@ -313,6 +332,7 @@ __global__ void pair_scatter_kernel(const CountParams P, int32_t* cursor, int32_
             }
         }
     }
+    (void)status;
 }
 
 // Warp-cooperative binary-search intersection count of two sorted lists in
@@ -1734,10 +1754,11 @@ __device__ __forceinline__ double hll_estimate_from(U128 zsum, double extra, uin
 // the FP64 comparison) proves the estimator takes its linear-counting
 // branch: E = m * ln(m / V), the same expression the full estimator
 // evaluates, and Z is not needed.  Otherwise pass 2 forms Z exactly and
-// applies the full estimator; the whole warp runs pass 2 for one such edge
-// at a time (coalesced loads, no lane idling while one group reads two
-// whole rows), so narrow groups cost nothing when a few of their edges need
-// the registers.
+// applies the full estimator.  For rows of at least 32 16-byte words
+// (p >= 9) the whole warp runs pass 2 for one such edge at a time
+// (coalesced loads, no lane idling while one group reads two whole rows),
+// so narrow groups cost nothing when a few of their edges need the
+// registers; smaller rows are read by the edge's own group.
 // CACHE: each group takes a contiguous run of the edge list.  The routing
 // pass appends edges in CSR order, so consecutive HLL edges mostly share u,
 // and the group keeps u's zero mask in registers across them (up to four
@@ -1824,30 +1845,43 @@ __global__ void __launch_bounds__(256, CROW ? 2 : (CACHE ? 3 : 4)) hll_edges_ker
         const bool need = act && zeros < H.lc_min;  // group-uniform
         double E = 0.0;
         if (act && !need) E = (double)m * log((double)m / (double)zeros);
-        if (CROW) {
-            if (need) {  // the group forms Z itself, u's row kept in registers
+        // rows of fewer than 32 16-byte words (p <= 8) would leave most of
+        // the warp idle in a warp-wide pass 2: there each group forms Z
+        if (CROW || nvec < 32) {
+            if (need) {  // the group forms Z itself (CROW: u's row kept in registers)
                 uint32_t fast = 0, zz = 0;
                 uint64_t fine = 0;
                 double extra = 0.0;
                 const uint4* a4 = reinterpret_cast<const uint4*>(H.regs + su * (int64_t)m);
                 const uint4* b4 = reinterpret_cast<const uint4*>(H.regs + sv * (int64_t)m);
-                if (su != cached_row) {  // group-uniform
+                if (CROW) {
+                    if (su != cached_row) {  // group-uniform
+#pragma unroll
+                        for (int kk = 0; kk < 8; ++kk) {
+                            const int i = sub + kk * L;
+                            ra[kk] = i < nvec ? __ldg(a4 + i) : make_uint4(0u, 0u, 0u, 0u);
+                        }
+                        cached_row = su;
+                    }
 #pragma unroll
                     for (int kk = 0; kk < 8; ++kk) {
                         const int i = sub + kk * L;
-                        ra[kk] = i < nvec ? __ldg(a4 + i) : make_uint4(0u, 0u, 0u, 0u);
+                        if (i < nvec) {
+                            const uint4 b = __ldg(b4 + i);
+                            hll_word_lut(__vmaxu4(ra[kk].x, b.x), S, fast, fine, zz, extra);
+                            hll_word_lut(__vmaxu4(ra[kk].y, b.y), S, fast, fine, zz, extra);
+                            hll_word_lut(__vmaxu4(ra[kk].z, b.z), S, fast, fine, zz, extra);
+                            hll_word_lut(__vmaxu4(ra[kk].w, b.w), S, fast, fine, zz, extra);
+                        }
                     }
-                    cached_row = su;
-                }
-#pragma unroll
-                for (int kk = 0; kk < 8; ++kk) {
-                    const int i = sub + kk * L;
-                    if (i < nvec) {
-                        const uint4 b = __ldg(b4 + i);
-                        hll_word_lut(__vmaxu4(ra[kk].x, b.x), S, fast, fine, zz, extra);
-                        hll_word_lut(__vmaxu4(ra[kk].y, b.y), S, fast, fine, zz, extra);
-                        hll_word_lut(__vmaxu4(ra[kk].z, b.z), S, fast, fine, zz, extra);
-                        hll_word_lut(__vmaxu4(ra[kk].w, b.w), S, fast, fine, zz, extra);
+                } else {
+#pragma unroll 2
+                    for (int i = sub; i < nvec; i += L) {
+                        const uint4 a = __ldg(a4 + i), b = __ldg(b4 + i);
+                        hll_word_lut(__vmaxu4(a.x, b.x), S, fast, fine, zz, extra);
+                        hll_word_lut(__vmaxu4(a.y, b.y), S, fast, fine, zz, extra);
+                        hll_word_lut(__vmaxu4(a.z, b.z), S, fast, fine, zz, extra);
+                        hll_word_lut(__vmaxu4(a.w, b.w), S, fast, fine, zz, extra);
                     }
                 }
                 fast = group_sum_u32<L>(fast, gmask);
@@ -2467,7 +2501,11 @@ class SideFork {
     std::unique_lock<std::mutex> lock_;
 };
 
-static int run_count(CountParams P, int mode, bool details, void* ws, size_t ws_bytes, cudaStream_t st) {
+// col_ready (exact counts only; null = ready): an event the kernels that
+// read col_idx wait for, so the pair regrouping (row_ptr and the edges only)
+// overlaps a copy of col_idx still in flight.
+static int run_count(CountParams P, int mode, bool details, void* ws, size_t ws_bytes, cudaStream_t st,
+                     cudaEvent_t col_ready = nullptr) {
     const Tuning T = tuning_snapshot();
     CountWs W;
     HybridWs HW{};
@@ -2503,6 +2541,10 @@ static int run_count(CountParams P, int mode, bool details, void* ws, size_t ws_
     P.hll_n = nullptr;
     if (P.n_edges == 0) return TCHLL_OK;
     const bool pairs = T.pairs && !details;
+    if (col_ready && !(mode == MODE_EXACT && pairs)) {
+        TCHLL_CUDA(cudaStreamWaitEvent(st, col_ready, 0));
+        col_ready = nullptr;
+    }
     int rc;
     CountParams Q;
     PhaseScope ps;
@@ -2522,12 +2564,17 @@ static int run_count(CountParams P, int mode, bool details, void* ws, size_t ws_
                 const bool side = hub > 0 && T.overlap && hub_pad_usable(P, W);
                 if (side) {
                     rc = fork.begin(st);
+                    if (rc == TCHLL_OK && col_ready) {
+                        const cudaError_t e = cudaStreamWaitEvent(fork.stream(), col_ready, 0);
+                        if (e != cudaSuccess) rc = cuda_status(e, "cudaStreamWaitEvent(col_ready)");
+                    }
                     if (rc == TCHLL_OK) rc = launch_core_pass(P, W, T, ps, fork.stream());
                     if (rc == TCHLL_OK) rc = fork.mark();
                     if (rc) return rc;
                 }
                 rc = pairs_scatter<false>(P, W, hub, Q, st);
                 if (rc) return rc;
+                if (col_ready) TCHLL_CUDA(cudaStreamWaitEvent(st, col_ready, 0));
                 phase_mark(ps, 1, st);
                 rc = launch_count<MODE_EXACT>(Q, T, false, st);
                 if (rc == TCHLL_OK && hub > 0) {
@@ -2673,6 +2720,26 @@ TCHLL_EXPORT int tchll_exact_count(const int32_t* row_ptr, int64_t n_nodes, cons
     P.result = result;
     P.p = 4;
     return run_count(P, MODE_EXACT, per_edge_support != nullptr, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+TCHLL_EXPORT int tchll_exact_count_staged(const int32_t* row_ptr, int64_t n_nodes, const int32_t* col_idx,
+                                          int64_t nnz, const int32_t* edge_u, const int32_t* edge_v,
+                                          int64_t n_edges, tchll_count_result* result, void* workspace,
+                                          size_t workspace_bytes, void* col_ready_event, void* stream) {
+    int rc = check_common(row_ptr, n_nodes, col_idx, nnz, edge_u, edge_v, n_edges, result);
+    if (rc) return rc;
+    CountParams P{};
+    P.row_ptr = row_ptr;
+    P.n_nodes = n_nodes;
+    P.col_idx = col_idx;
+    P.nnz = nnz;
+    P.edge_u = edge_u;
+    P.edge_v = edge_v;
+    P.n_edges = n_edges;
+    P.result = result;
+    P.p = 4;
+    return run_count(P, MODE_EXACT, false, workspace, workspace_bytes, (cudaStream_t)stream,
+                     (cudaEvent_t)col_ready_event);
 }
 
 static int hybrid_common(const int32_t* row_ptr, int64_t n_nodes, const int32_t* col_idx, int64_t nnz,

@@ -66,11 +66,33 @@ def _inputs(row_ptr_d, col_idx_d, edge_u_d, edge_v_d):
     return rp, ci, eu, ev
 
 
+def _is_host(x) -> bool:
+    if isinstance(x, torch.Tensor):
+        return not x.is_cuda
+    return not hasattr(x, "__cuda_array_interface__")
+
+
 def gpu_exact_triangle_count(row_ptr_d, col_idx_d, edge_u_d, edge_v_d):
     """Exact count over the given oriented edges; returns ``(count, elapsed_s)``
     where elapsed is the wall-clock time of the synchronised launch, as in the
-    reference (src/gpu_hybrid.py:346-354)."""
+    reference (src/gpu_hybrid.py:346-354).  Host arrays (all four) are copied
+    in stages that overlap the count (``core.exact_count_host``), and elapsed
+    then runs from the first copy to the result."""
     _require_supported_block_size()
+    if all(_is_host(x) for x in (row_ptr_d, col_idx_d, edge_u_d, edge_v_d)):
+        _lib.require_cuda()
+        host = [x if isinstance(x, torch.Tensor) else torch.as_tensor(x)
+                for x in (row_ptr_d, col_idx_d, edge_u_d, edge_v_d)]
+        dev = torch.device("cuda", torch.cuda.current_device())
+        with torch.cuda.device(dev):
+            res = _lib.count_result_tensor(dev)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            core.exact_count_host(*host, device=dev, result=res)
+            torch.cuda.synchronize()
+            elapsed = time.perf_counter() - t0
+            count = core.exact_from_result(res)
+        return count, elapsed
     rp, ci, eu, ev = _inputs(row_ptr_d, col_idx_d, edge_u_d, edge_v_d)
     with torch.cuda.device(rp.device):
         res = _lib.count_result_tensor(rp.device)

@@ -70,6 +70,7 @@ class Completion:
     stats: Optional[Dict] = None
     latency: float = float("nan")
     error: Optional[str] = None
+    device_ms: float = float("nan")  # answer_alone: device time from generation to the result
 
 
 def c5_requests(n: int, rate_per_s: float, seed: int = 0, scale_range=(12, 20), ef_range=(8, 32),
@@ -513,7 +514,11 @@ def serve_sequential(requests: Sequence[Request], device=None) -> List[Completio
 
 
 def answer_alone(r: Request, dev, t0: Optional[float] = None) -> Completion:
-    """One query on its own: the plain per-graph path."""
+    """One query on its own: the plain per-graph path.  ``device_ms`` is the
+    CUDA-event time from the graph's generation to its result (the device
+    work of one query, with the build's one size read-back inside)."""
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
     u, v = generate_edges(r, dev)
     g = core.csr_from_edges(u, v, device=dev)
     del u, v
@@ -528,17 +533,26 @@ def answer_alone(r: Request, dev, t0: Optional[float] = None) -> Completion:
                                                    r.p, r.gamma, split_kernels=True)
         val, rr = core.hybrid_from_result(res)
         st = {k: int(getattr(rr, k)) for k in ("n_approx", "n_exact", "n_fallback", "n_clamped")}
+    e1.record()
     lat = (time.perf_counter() - t0 - r.arrival) if t0 is not None else float("nan")
-    return Completion(r.rid, r.mode, val, st, latency=lat)
+    e1.synchronize()
+    return Completion(r.rid, r.mode, val, st, latency=lat, device_ms=e0.elapsed_time(e1))
 
 
 def latency_summary(done: Sequence[Completion], wall_s: float) -> Dict:
     ok = [c for c in done if c.error is None]
     lat = np.array([c.latency for c in ok]) * 1e3
-    return {"completed": len(ok), "errors": len(done) - len(ok),
-            "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
-            "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
-            "graphs_per_s": len(ok) / wall_s if wall_s > 0 else None}
+    out = {"completed": len(ok), "errors": len(done) - len(ok),
+           "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
+           "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
+           "graphs_per_s": len(ok) / wall_s if wall_s > 0 else None}
+    dms = np.array([c.device_ms for c in ok if c.device_ms == c.device_ms])
+    if len(dms):  # one query at a time: the device work behind each answer
+        out["device_ms_total"] = float(dms.sum())
+        out["device_ms_mean"] = float(dms.mean())
+        out["device_bound_graphs_per_s"] = float(len(dms) / (dms.sum() / 1e3)) if dms.sum() > 0 else None
+        out["device_busy_frac"] = float(dms.sum() / 1e3 / wall_s) if wall_s > 0 else None
+    return out
 
 
 def _warm(dev) -> None:
