@@ -215,6 +215,9 @@ def phase_report(pair_ms, count_ms, hub_ms, core_ms, tuning: dict) -> dict:
     out = {"pair_regroup": pair_ms, "count": count_ms, "hub_kernels": hub_ms}
     if not hub_ms:
         out["pair_kernel"] = count_ms
+    elif tuning.get("overlap", 0) >= 2:  # the short-list pairs run on the second stream too
+        out["hub_core_pass_beside"] = core_ms
+        out["core_wait"] = count_ms - hub_ms
     elif tuning.get("overlap"):
         out["hub_core_pass_beside"] = core_ms
         out["pair_kernel_and_core_wait"] = count_ms - hub_ms

@@ -176,9 +176,11 @@ int tchll_get_count_hub(int32_t* out4 /* host */);
  * hold 16-bit core indices (two planes) and the bitmap takes 16 KB; else,
  * when the core fits 8 * 2^bitmap_log2 bits (minus 32), 32-bit lists and a
  * bitmap of that size; else hash tables.  bitmap_log2 0 turns the 32-bit
- * bitmap off; otherwise in [10, 17].  overlap != 0 runs the hub core pass
- * and a hybrid count's HLL pass on a second stream beside the exact pairs
- * (joined before the call returns).  bank_sort != 0 orders each packed
+ * bitmap off; otherwise in [10, 17].  overlap 1 runs the hub core pass
+ * and a hybrid count's HLL pass on a second stream beside the exact pairs;
+ * overlap 2 also moves an exact count's short-list pair kernel there, after
+ * the core pass, beside the hub kernel; 0 runs everything on the caller's
+ * stream (the second stream is joined before the call returns).  bank_sort != 0 orders each packed
  * list's keys by the shared-memory bank of their bitmap word (fewer bank
  * conflicts in the hub kernel, a slower core pass).  out4 receives the four
  * values.  Results are identical for every setting.  These kernels read

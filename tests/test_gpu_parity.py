@@ -368,7 +368,8 @@ def test_hub_core_bitmap_hash_and_overlap_match_oracle(tchll, oracle, dev):
     16 KB bitmap, 32-bit lists with a bitmap of the configured size (core
     fits), hash tables only (bitmap off), a bitmap buffer too small for the
     core (the bitmap kernel steps aside on the device and the hash kernel
-    counts), each with the hybrid's HLL pass on the side stream or inline:
+    counts), each with the hybrid's HLL pass on the side stream or inline
+    (overlap 2: the exact count's short-list pairs on the side stream too):
     exact counts and hybrid result blocks identical and equal to the oracle.
     (Two-plane packed lists, a core above 65,535 vertices, run in the R-MAT
     scale-22 test.)"""
@@ -392,10 +393,11 @@ def test_hub_core_bitmap_hash_and_overlap_match_oracle(tchll, oracle, dev):
     blocks = []
     try:
         for hub, blg, ov, pk in ((128, 15, 1, 1), (128, 15, 1, 0), (128, 0, 1, 0), (64, 10, 0, 0), (64, 15, 0, 1),
-                                 (128, 12, 1, 0), (200, 17, 1, 0), (64, 0, 0, 1), (128, 0, 1, 2), (64, 0, 0, 2)):
+                                 (128, 12, 1, 0), (200, 17, 1, 0), (64, 0, 0, 1), (128, 0, 1, 2), (64, 0, 0, 2),
+                                 (128, 15, 2, 1), (64, 0, 2, 0)):
             # pk 2: packed lists ordered by bitmap bank
             core.set_count_tuning(base["chunk"], base["slots_log2"], base["tiny"], base["blocks_per_sm"], hub=hub,
-                                  bitmap_lg=blg, overlap=bool(ov), packed=bool(pk), bank_sort=pk == 2)
+                                  bitmap_lg=blg, overlap=ov, packed=bool(pk), bank_sort=pk == 2)
             assert core.get_count_tuning()["bitmap_lg"] == blg
             assert _exact(core, g) == want, (hub, blg, ov, pk)
             res, _ = core.hybrid_count_compact_tensors(g.row_ptr, g.col_idx, g.edge_u, g.edge_v, g.degrees, rows,

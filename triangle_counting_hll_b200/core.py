@@ -297,15 +297,17 @@ def set_count_tuning(chunk: int = 256, slots_log2: int = 10, tiny: int = 16, blo
                      warps: Optional[int] = None, pairs: Optional[bool] = None,
                      sparse: Optional[bool] = None, hub: Optional[int] = None, hub_seg: Optional[int] = None,
                      hub_lg: Optional[int] = None, hub_unroll: Optional[int] = None,
-                     bitmap_lg: Optional[int] = None, overlap: Optional[bool] = None,
+                     bitmap_lg: Optional[int] = None, overlap: Optional[int] = None,
                      packed: Optional[bool] = None, bank_sort: Optional[bool] = None,
                      hll_row_cache_p: Optional[int] = None, hll_lanes: Optional[int] = None) -> None:
     """Launch shape of the counting kernels (results do not depend on it).
     hub / hub_seg / hub_lg / hub_unroll: threshold on d+(x) above which a pair
     goes to the CTA-shared table kernels (0: off), pairs per work unit, log2
     hash-table slots, probe loads in flight per lane.  bitmap_lg: log2 bytes
-    of the 32-bit hub bitmap buffer (0: off); overlap: hybrid HLL pass on a
-    second stream beside the exact pairs; packed: 16-bit hub probe lists when
+    of the 32-bit hub bitmap buffer (0: off); overlap: 0 one stream, 1 the
+    hub core pass (and a hybrid's HLL pass) on a second stream beside the
+    exact pairs, 2 also the short-list pair kernel there, beside the hub
+    kernel; packed: 16-bit hub probe lists when
     the core has at most 131,070 vertices; bank_sort: packed lists ordered by
     bitmap bank.  hll_row_cache_p / hll_lanes:
     the HLL pass's one-pass threshold on p and lanes per edge (0: by p)."""
@@ -314,7 +316,7 @@ def set_count_tuning(chunk: int = 256, slots_log2: int = 10, tiny: int = 16, blo
     check(L.tchll_set_hll_pass(int(cur["hll_row_cache_p"] if hll_row_cache_p is None else hll_row_cache_p),
                                int(cur["hll_lanes"] if hll_lanes is None else hll_lanes)))
     check(L.tchll_set_count_core(int(cur["bitmap_lg"] if bitmap_lg is None else bitmap_lg),
-                                 int(cur["overlap"] if overlap is None else bool(overlap)),
+                                 int(cur["overlap"] if overlap is None else int(overlap)),
                                  int(cur["packed"] if packed is None else bool(packed)),
                                  int(cur["bank_sort"] if bank_sort is None else bool(bank_sort))))
     check(L.tchll_set_count_hub(int(cur["hub"] if hub is None else hub),

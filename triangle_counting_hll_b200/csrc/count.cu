@@ -910,8 +910,12 @@ __global__ void __launch_bounds__(256) core_pad16_kernel(const int32_t* __restri
                 hi = t < 8 ? lo + (int32_t)(((t + 1) * len) / 9) : hi;
                 lo = nlo;
             }
-            int c = 0;
-            for (int32_t m = lo + sub; m < hi; m += 8) c += __ldg(col + rs + m) < wsplit;
+            int c = 0;  // hi - lo <= 64: eight independent loads per lane
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+                const int32_t m = lo + sub + 8 * t;
+                if (m < hi) c += __ldg(col + rs + m) < wsplit;
+            }
             c += __shfl_xor_sync(gmask, c, 1);
             c += __shfl_xor_sync(gmask, c, 2);
             c += __shfl_xor_sync(gmask, c, 4);
@@ -1398,19 +1402,19 @@ __global__ void __launch_bounds__(256, 6) hub_bitmap_kernel(const HubParams H) {
 // half the bytes.  The bitmap has 65,536 bits (C <= 65535) or 131,072 bits
 // (16 KB of shared memory); a unit's plane (the bitmap's half) follows from
 // its position in the list: units at or past the list's plane-0 units are
-// plane 1.  Otherwise as hub_bitmap_kernel.
+// plane 1.  The bitmap is built from x's own packed list (16-byte loads of 8
+// keys; x's members are the core's by construction, so no member can miss
+// and there is no binary-search fallback).  Otherwise as hub_bitmap_kernel.
 template <int UNR>
 __global__ void __launch_bounds__(256, 8) hub_bitmap16_kernel(const HubParams H) {
     extern __shared__ __align__(16) uint32_t bm[];  // 4096 words
     __shared__ HubSeg s_seg;
     __shared__ int s_round;
-    __shared__ int s_fail;
     const int C = H.n_core[0];
     if (!H.packed || C > kCore16Max) return;  // grid-uniform: a 32-bit kernel counts
     const int tid = threadIdx.x, lane = tid & 31;
     const unsigned lane_le = (2u << lane) - 1u;
     const int nw4 = C > kPlane ? 1024 : 512;  // uint4 words: 131,072 or 65,536 bits
-    const int32_t* __restrict__ col = H.col_idx;
     const uint4* __restrict__ pq = reinterpret_cast<const uint4*>(H.pcol);
     const int64_t nseg = min((int64_t)*H.n_segs, H.max_segs);
     uint64_t acc = 0;
@@ -1426,27 +1430,29 @@ __global__ void __launch_bounds__(256, 8) hub_bitmap16_kernel(const HubParams H)
                 s_seg.start = 0;
             }
             s_round = 0;
-            s_fail = 0;
         }
         for (int i = tid; i < nw4; i += blockDim.x) reinterpret_cast<uint4*>(bm)[i] = make_uint4(0u, 0u, 0u, 0u);
         __syncthreads();
         const HubSeg sg = s_seg;
         if (sg.x < 0) break;
         if (tid == 0) n_pairs += sg.len;
-        const int32_t xs = __ldg(H.row_ptr + sg.x);
-        const int xl = __ldg(H.row_ptr + sg.x + 1) - xs;
-        for (int i = tid; i < xl; i += blockDim.x) {
-            const int32_t w = __ldg(col + xs + i);
-            const int32_t c = (uint64_t)(uint32_t)w < (uint64_t)H.n_nodes ? __ldg(H.cidx + w) : -1;
-            if (c >= 0) {
-                const int32_t bit = c < kPlane ? c : c + 1;
-                atomicOr(bm + (bit >> 5), 1u << (bit & 31));
-            } else {
-                s_fail = 1;  // not in the core (cannot happen for well-formed input)
+        {
+            // N+(x) from x's own packed list (x's members are the core's by
+            // construction): 8 keys per 16-byte load, padding skipped;
+            // plane-1 key k is core index k + kPlane, bit k + kPlane + 1
+            const int4 xr = H.pl[sg.x];
+            for (int i = tid; i < xr.z; i += blockDim.x) {
+                const uint4 q = __ldg(pq + xr.x + i);
+                const uint32_t hb = i >= xr.y ? 65536u : 0u;
+                const uint32_t w4[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+                for (int t = 0; t < 8; ++t) {
+                    const uint32_t k = (w4[t >> 1] >> (16 * (t & 1))) & 0xFFFFu;
+                    if (k != 0xFFFFu) atomicOr(bm + ((k + hb) >> 5), 1u << (k & 31));
+                }
             }
         }
         __syncthreads();
-        const bool table = !s_fail;  // CTA-uniform
         int rsz = (sg.len + 15) >> 4;
         rsz = rsz < 4 ? 4 : (rsz > 32 ? 32 : rsz);
         while (true) {
@@ -1455,21 +1461,12 @@ __global__ void __launch_bounds__(256, 8) hub_bitmap16_kernel(const HubParams H)
             r = __shfl_sync(FULL, r, 0);
             if (r >= sg.len) break;
             const int np = min(rsz, sg.len - r);
-            int32_t y = 0, q0 = 0, nq = 0, lo = 0;
+            int32_t q0 = 0, nq = 0, lo = 0;
             if (lane < np) {
-                y = __ldg(H.hy + sg.start + r + lane);
-                const int4 u = H.pl[y];
+                const int4 u = H.pl[__ldg(H.hy + sg.start + r + lane)];
                 q0 = u.x;
                 lo = u.y;
                 nq = u.z;
-            }
-            if (!table) {  // binary search per pair over the raw lists
-                for (int j = 0; j < np; ++j) {
-                    const int32_t yj = __shfl_sync(FULL, y, j);
-                    const int32_t jrs = __ldg(H.row_ptr + yj), jre = __ldg(H.row_ptr + yj + 1);
-                    acc += warp_bsearch_count(col + xs, xl, col + jrs, jre - jrs, lane);
-                }
-                continue;
             }
             const unsigned ne = __ballot_sync(FULL, nq > 0);
             const int k = __popc(ne);
@@ -1972,7 +1969,7 @@ struct Tuning {
     int hub_lg = 13;        // largest CTA hash table: 2^13 slots = 32 KB
     int hub_unroll = 2;     // quads per lane in flight (2 or 4)
     int bitmap_lg = 15;     // hub bitmap buffer: 2^15 bytes = 262,144 core vertices (0: hash tables only)
-    int overlap = 1;        // hybrid: HLL pass on a side stream beside the exact pairs
+    int overlap = 1;        // side stream: 1 the hub core pass (+ the hybrid HLL pass); 2 also the short-list pairs
     int packed = 1;         // hub probe lists as 16-bit core indices when the core allows
     int bank_sort = 0;      // packed lists ordered by bitmap bank within each plane
     int hll_row_cache_p = 0;   // HLL pass: keep u's register row in registers for p <= this (0: never)
@@ -2441,7 +2438,7 @@ static int hub_threshold(const CountParams& P, const Tuning& T) {
 // capture: the first call of a process is never captured by this package).
 struct SideStream {
     cudaStream_t s = nullptr;
-    cudaEvent_t fork = nullptr, mid = nullptr, join = nullptr;
+    cudaEvent_t fork = nullptr, mid = nullptr, join = nullptr, back = nullptr;
     std::mutex mu;
 };
 static SideStream g_side[kMaxDevices];
@@ -2462,6 +2459,7 @@ class SideFork {
                 TCHLL_CUDA(cudaEventCreateWithFlags(&S.fork, cudaEventDisableTiming));
                 TCHLL_CUDA(cudaEventCreateWithFlags(&S.mid, cudaEventDisableTiming));
                 TCHLL_CUDA(cudaEventCreateWithFlags(&S.join, cudaEventDisableTiming));
+                TCHLL_CUDA(cudaEventCreateWithFlags(&S.back, cudaEventDisableTiming));
             }
         }
         lock_ = std::unique_lock<std::mutex>(S.mu);
@@ -2480,6 +2478,12 @@ class SideFork {
     }
     int wait_mark() {
         TCHLL_CUDA(cudaStreamWaitEvent(caller_, side_->mid, 0));
+        return TCHLL_OK;
+    }
+    // The side stream waits for the caller's work so far (once per fork).
+    int side_waits_caller() {
+        TCHLL_CUDA(cudaEventRecord(side_->back, caller_));
+        TCHLL_CUDA(cudaStreamWaitEvent(side_->s, side_->back, 0));
         return TCHLL_OK;
     }
     // Joins: the caller's stream waits for everything enqueued on the side
@@ -2576,10 +2580,19 @@ static int run_count(CountParams P, int mode, bool details, void* ws, size_t ws_
                 if (rc) return rc;
                 if (col_ready) TCHLL_CUDA(cudaStreamWaitEvent(st, col_ready, 0));
                 phase_mark(ps, 1, st);
-                rc = launch_count<MODE_EXACT>(Q, T, false, st);
-                if (rc == TCHLL_OK && hub > 0) {
-                    rc = side ? fork.wait_mark() : launch_core_pass(P, W, T, ps, st);
+                if (side && T.overlap >= 2) {
+                    // the short-list pairs follow the core pass on the side
+                    // stream (once scattered) and run beside the hub kernel
+                    rc = fork.side_waits_caller();
+                    if (rc == TCHLL_OK) rc = launch_count<MODE_EXACT>(Q, T, false, fork.stream());
+                    if (rc == TCHLL_OK) rc = fork.wait_mark();
                     if (rc == TCHLL_OK) rc = launch_hub(P, W, T, ps, st);
+                } else {
+                    rc = launch_count<MODE_EXACT>(Q, T, false, st);
+                    if (rc == TCHLL_OK && hub > 0) {
+                        rc = side ? fork.wait_mark() : launch_core_pass(P, W, T, ps, st);
+                        if (rc == TCHLL_OK) rc = launch_hub(P, W, T, ps, st);
+                    }
                 }
                 phase_mark(ps, 2, st);
                 const int rj = fork.end();
@@ -2862,7 +2875,8 @@ TCHLL_EXPORT int tchll_set_count_core(int32_t bitmap_log2, int32_t overlap, int3
     TCHLL_ARG(bitmap_log2 == 0 || (bitmap_log2 >= 10 && bitmap_log2 <= 17),
               "bitmap_log2 must be 0 (hash tables only) or in [10, 17] (1 KB .. 128 KB of shared memory)");
     g_tuning.bitmap_lg = bitmap_log2;
-    g_tuning.overlap = overlap ? 1 : 0;
+    TCHLL_ARG(overlap >= 0 && overlap <= 2, "overlap must be 0, 1 or 2");
+    g_tuning.overlap = overlap;
     g_tuning.packed = packed ? 1 : 0;
     g_tuning.bank_sort = bank_sort ? 1 : 0;
     return TCHLL_OK;

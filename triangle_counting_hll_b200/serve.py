@@ -29,6 +29,7 @@ from __future__ import annotations
 import collections
 import math
 import queue
+import sys
 import threading
 import time
 from dataclasses import dataclass, field
@@ -472,7 +473,11 @@ class Server:
         self._est: Dict[Tuple, int] = {}
         self.pending = []
         self._worker = _BuildWorker(self.dev, self.build_stream, self.big_edges)
+        switch = sys.getswitchinterval()
         if self.threaded:
+            # the worker needs the interpreter lock back after each CUDA call
+            # it waits in: hand it over within 0.5 ms instead of 5 ms
+            sys.setswitchinterval(min(switch, 5e-4))
             self._worker.start()
         self._t0 = t0 = time.perf_counter()
         i = 0
@@ -491,10 +496,13 @@ class Server:
                 if not busy:  # nothing to do until an arrival, a build or a count finishes
                     nxt = reqs[i].arrival - (time.perf_counter() - t0) if i < len(reqs) else 1.0
                     time.sleep(max(0.0, min(nxt, 0.0002)))
+                elif self.threaded:
+                    time.sleep(0)  # let the build worker take the interpreter lock
         finally:
             if self.threaded:
                 self._worker.inbox.put(None)
                 self._worker.join(timeout=60)
+                sys.setswitchinterval(switch)
         return sorted(self._done, key=lambda c: c.rid)
 
 
