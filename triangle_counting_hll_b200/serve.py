@@ -231,13 +231,9 @@ class Server:
 
     def __init__(self, device=None, budget_bytes: float = 120e9, max_batch: int = 256,
                  max_batch_edges: float = 4e8, big_edges: int = 1 << 20, threaded: bool = True,
-                 reserve_pools: bool = False, defer_backlog: int = 8):
+                 reserve_pools: bool = False):
         self.dev = core._device(device)
         self.threaded = threaded  # builds on a worker thread (True) or on the serving loop (False)
-        # a new large graph waits for the large graph in flight while at most
-        # this many requests are waiting (0: never waits)
-        self.defer_backlog = int(defer_backlog)
-        self._deferred: "collections.deque[Request]" = collections.deque()
         self.big_edges = int(big_edges)
         self.budget = int(budget_bytes)
         self.max_batch = max_batch
@@ -276,13 +272,6 @@ class Server:
                 del block
             free, _ = torch.cuda.mem_get_info(self.dev)
 
-    def _big_busy(self) -> bool:
-        """Is a large graph being built, or a large graph's count in flight?"""
-        for reqs in self.building.values():
-            if reqs and reqs[0].raw_edges() >= self.big_edges:
-                return True
-        return any(len(it[1]) == 1 and it[1][0].raw_edges() >= self.big_edges for it in self.pending)
-
     def _evict_for(self, need: int, pinned: set) -> bool:
         while self.resident_bytes + self.inflight_bytes + need > self.budget:
             victim = next((k for k in self.resident
@@ -304,22 +293,8 @@ class Server:
         pinned: set = set()
         edges = 0
         taken = 0
-        big_busy = self._big_busy()
-        if self._deferred:
-            if not big_busy:  # the oldest deferred large graph goes next
-                queue_.appendleft(self._deferred.popleft())
-            elif len(queue_) + len(self._deferred) > self.defer_backlog:  # saturated: no more waiting
-                while self._deferred:
-                    queue_.appendleft(self._deferred.pop())
         while queue_ and taken < self.max_batch:
             r = queue_[0]
-            if (big_busy and r.raw_edges() >= self.big_edges and r.key not in self.building
-                    and r.key not in self.resident and len(queue_) + len(self._deferred) <= self.defer_backlog):
-                # below saturation a large graph waits until the large graph
-                # on the GPU is answered: overlapping two large graphs' builds
-                # and counts only lengthens both; small graphs go past it
-                self._deferred.append(queue_.popleft())
-                continue
             if r.key in self.building:  # its graph is being built: answer it with that build
                 queue_.popleft()
                 self.building[r.key].append(r)
@@ -362,7 +337,6 @@ class Server:
                 small_job.append((r.key, r, None))
             else:
                 jobs.append([(r.key, r, None)])
-                big_busy = True
             edges += r.raw_edges()
             taken += 1
         if small_job:  # small graphs: one job, then one batched launch
@@ -523,7 +497,6 @@ class Server:
         self._done = []
         self._est: Dict[Tuple, int] = {}
         self.pending = []
-        self._deferred = collections.deque()
         self._worker = _BuildWorker(self.dev, self.build_stream, self.big_edges)
         switch = sys.getswitchinterval()
         if self.threaded:
@@ -541,7 +514,7 @@ class Server:
                     i += 1
                 busy = self._reap()
                 busy |= self._collect()
-                ready = self._admit(queue_, self._done, now) if (queue_ or self._deferred) else []
+                ready = self._admit(queue_, self._done, now) if queue_ else []
                 if ready:
                     self._launch_all(ready)
                     busy = True
