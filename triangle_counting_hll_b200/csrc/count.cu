@@ -229,13 +229,6 @@ __device__ __forceinline__ void lane_runs(int32_t key, int lane, int& head_lane,
     run_len = (after ? __ffs(after) - 1 : 32) - head_lane;
 }
 
-// Grid-stride loop that whole warps enter and leave together: e may reach
-// past n in the last pass; the body tests it.
-#define WARP_EDGE_LOOP(e, n)                                                                   \
-    for (int64_t _wb = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31u),                \
-                 e = _wb + (threadIdx.x & 31u);                                                \
-         _wb < (n); _wb += (int64_t)gridDim.x * blockDim.x, e = _wb + (threadIdx.x & 31u))
-
 // er[e] (the histogram's record of edge e for the scatter): -1 when the edge
 // makes no exact pair (malformed, or HLL-routed), else the pair's rank in its
 // table side's bucket, with bit 31 set when the table side is v.  A bucket
@@ -247,48 +240,70 @@ __global__ void pair_hist_kernel(const CountParams P, int32_t* cnt, uint32_t* er
     uint32_t status = 0;
     unsigned long long fallback = 0;
     const int lane = threadIdx.x & 31;
-    WARP_EDGE_LOOP(e, P.n_edges) {
-        int32_t u = 0, v = 0, us = 0, ue = 0, vs = 0, ve = 0;
-        bool ok = e < P.n_edges && load_edge(P, e, u, v, us, ue, vs, ve, status);
-        bool hll = false;
-        if (HYB && ok) {
-            int32_t du, dv;
-            int64_t su, sv;
-            bool wants, both;
-            ok = route(P, u, v, du, dv, su, sv, wants, both, status);
-            hll = ok && wants && both;
-            if (ok && wants && !both) {
-                if (P.graph_vbase && P.hll_u)  // batched: this edge's graph
-                    atomicAdd((unsigned long long*)&P.result[graph_of(P.graph_vbase, P.n_graphs, u)].n_fallback, 1ull);
-                else
-                    ++fallback;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    // two warp-wide steps per pass, their loads and rank claims interleaved:
+    // each step is a chain of dependent loads and a returning atomic
+    constexpr int K = 2;
+    for (int64_t wb = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31u); wb < P.n_edges; wb += K * stride) {
+        int32_t u[K], v[K], us[K], ue[K], vs[K], ve[K];
+        bool ok[K], hll[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int64_t e = wb + k * stride + lane;
+            u[k] = v[k] = us[k] = ue[k] = vs[k] = ve[k] = 0;
+            ok[k] = e < P.n_edges && load_edge(P, e, u[k], v[k], us[k], ue[k], vs[k], ve[k], status);
+            hll[k] = false;
+            if (HYB && ok[k]) {
+                int32_t du, dv;
+                int64_t su, sv;
+                bool wants, both;
+                ok[k] = route(P, u[k], v[k], du, dv, su, sv, wants, both, status);
+                hll[k] = ok[k] && wants && both;
+                if (ok[k] && wants && !both) {
+                    if (P.graph_vbase && P.hll_u)  // batched: this edge's graph
+                        atomicAdd((unsigned long long*)&P.result[graph_of(P.graph_vbase, P.n_graphs, u[k])].n_fallback,
+                                  1ull);
+                    else
+                        ++fallback;
+                }
             }
         }
-        {
-            // a run of lanes with the same table side claims its ranks with
-            // one atomic; each lane records its rank for the scatter
-            const bool counted = ok && !hll;
-            const bool side_u = (ue - us) >= (ve - vs);
-            const int32_t x = counted ? (side_u ? u : v) : -1 - lane;
-            int head, len;
-            lane_runs(x, lane, head, len);
-            int32_t base = 0;
-            if (counted && lane == head) base = atomicAdd(cnt + x, len);
-            base = __shfl_sync(FULL, base, head);
+        // a run of lanes with the same table side claims its ranks with one
+        // atomic; each lane records its rank for the scatter
+        bool counted[K], side_u[K];
+        int32_t x[K], base[K];
+        int head[K], len[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            counted[k] = ok[k] && !hll[k];
+            side_u[k] = (ue[k] - us[k]) >= (ve[k] - vs[k]);
+            x[k] = counted[k] ? (side_u[k] ? u[k] : v[k]) : -1 - lane;
+            lane_runs(x[k], lane, head[k], len[k]);
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k) base[k] = (counted[k] && lane == head[k]) ? atomicAdd(cnt + x[k], len[k]) : 0;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int64_t e = wb + k * stride + lane;
+            base[k] = __shfl_sync(FULL, base[k], head[k]);
             if (e < P.n_edges)
-                er[e] = counted ? ((uint32_t)(base + (lane - head)) | (side_u ? 0u : kRankSideV)) : 0xFFFFFFFFu;
+                er[e] = counted[k] ? ((uint32_t)(base[k] + (lane - head[k])) | (side_u[k] ? 0u : kRankSideV))
+                                   : 0xFFFFFFFFu;
         }
         if (HYB && P.hll_u) {
-            // warp-aggregated append of the HLL-routed edges
-            const unsigned bal = __ballot_sync(FULL, hll);
-            if (bal) {
-                unsigned long long base = 0;
-                if (lane == 0) base = atomicAdd(P.hll_n, (unsigned long long)__popc(bal));
-                base = __shfl_sync(FULL, base, 0);
-                if (hll) {
-                    const unsigned long long pos = base + __popc(bal & ((1u << lane) - 1u));
-                    P.hll_u[pos] = u;
-                    P.hll_v[pos] = v;
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                // warp-aggregated append of the HLL-routed edges
+                const unsigned bal = __ballot_sync(FULL, hll[k]);
+                if (bal) {
+                    unsigned long long hb = 0;
+                    if (lane == 0) hb = atomicAdd(P.hll_n, (unsigned long long)__popc(bal));
+                    hb = __shfl_sync(FULL, hb, 0);
+                    if (hll[k]) {
+                        const unsigned long long pos = hb + __popc(bal & ((1u << lane) - 1u));
+                        P.hll_u[pos] = u[k];
+                        P.hll_v[pos] = v[k];
+                    }
                 }
             }
         }
