@@ -74,7 +74,7 @@ uint64_t tchll_launch_count(void);
 /* Workspace for tchll_exact_count / tchll_hybrid_count_* on a CSR of n_nodes
  * rows and n_edges edges: the regrouped pair lists, per-vertex histograms and
  * offsets, the long-list work units, 16-byte-aligned copies of the probe
- * lists and, for hybrid counts, the HLL edge list -- about 24 bytes per edge
+ * lists and, for hybrid counts, the HLL edge list -- about 20 bytes per edge
  * + 110 per vertex.  The aligned copies are optional: a workspace too small
  * for them but large enough otherwise runs without them (same results). */
 int tchll_count_workspace_bytes(int64_t n_nodes, int64_t n_edges, size_t* bytes);
@@ -205,10 +205,9 @@ int tchll_get_hll_pass(int32_t* out2 /* host */);
  * result as tchll_exact_count without per-edge output, but the scratch comes
  * from a fixed array of TCHLL_NOALLOC_SCRATCH_BYTES inside the library that
  * every GPU loading the library reserves until the process exits; graphs
- * needing more scratch (about 12 bytes per edge + 32 per vertex: the pair
- * lists and their ranks, four per-vertex histograms / offsets and the
- * work-unit list, so for example 2 M edges on 200 K vertices fit) are
- * rejected with TCHLL_EINVAL.
+ * needing more scratch (about 8 bytes per edge + 32 per vertex: the pair
+ * lists, four per-vertex histograms / offsets and the work-unit list, so for
+ * example 3 M edges on 200 K vertices fit) are rejected with TCHLL_EINVAL.
  * The first
  * call in each CUDA context looks up the array's device address (cached per
  * context id, so a context made current by the caller, or one re-created

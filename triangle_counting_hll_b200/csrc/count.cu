@@ -205,6 +205,24 @@ __device__ __forceinline__ bool route(const CountParams& P, int32_t u, int32_t v
 // ------------------------------------------------------------ pair build ----
 // Exact edges (all edges, or in hybrid mode the exact-routed ones) become
 // pairs (x, y), x the endpoint with the longer forward list (ties: u).
+template <bool HYB>
+__device__ __forceinline__ bool pair_of(const CountParams& P, int64_t e, int32_t& x, int32_t& y, int32_t& xl,
+                                        uint32_t& status) {
+    int32_t u, v, us, ue, vs, ve;
+    if (!load_edge(P, e, u, v, us, ue, vs, ve, status)) return false;
+    if (HYB) {
+        int32_t du, dv;
+        int64_t su, sv;
+        bool wants, both;
+        if (!route(P, u, v, du, dv, su, sv, wants, both, status)) return false;
+        if (wants && both) return false;  // HLL-routed
+    }
+    const bool ux = (ue - us) >= (ve - vs);
+    x = ux ? u : v;
+    y = ux ? v : u;
+    xl = ux ? (ue - us) : (ve - vs);
+    return true;
+}
 
 // Batched calls: the graph of vertex v, the last g with vbase[g] <= v.
 __device__ __forceinline__ int64_t graph_of(const int32_t* vbase, int64_t n_graphs, int32_t v) {
@@ -229,81 +247,54 @@ __device__ __forceinline__ void lane_runs(int32_t key, int lane, int& head_lane,
     run_len = (after ? __ffs(after) - 1 : 32) - head_lane;
 }
 
-// er[e] (the histogram's record of edge e for the scatter): -1 when the edge
-// makes no exact pair (malformed, or HLL-routed), else the pair's rank in its
-// table side's bucket, with bit 31 set when the table side is v.  A bucket
-// holds fewer than nnz < 2^31 pairs, so a rank never reaches bit 31.
-constexpr uint32_t kRankSideV = 0x80000000u;
+// Grid-stride loop that whole warps enter and leave together: e may reach
+// past n in the last pass; the body tests it.
+#define WARP_EDGE_LOOP(e, n)                                                                   \
+    for (int64_t _wb = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31u),                \
+                 e = _wb + (threadIdx.x & 31u);                                                \
+         _wb < (n); _wb += (int64_t)gridDim.x * blockDim.x, e = _wb + (threadIdx.x & 31u))
 
 template <bool HYB>
-__global__ void pair_hist_kernel(const CountParams P, int32_t* cnt, uint32_t* er) {
+__global__ void pair_hist_kernel(const CountParams P, int32_t* cnt) {
     uint32_t status = 0;
     unsigned long long fallback = 0;
     const int lane = threadIdx.x & 31;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    // two warp-wide steps per pass, their loads and rank claims interleaved:
-    // each step is a chain of dependent loads and a returning atomic
-    constexpr int K = 2;
-    for (int64_t wb = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31u); wb < P.n_edges; wb += K * stride) {
-        int32_t u[K], v[K], us[K], ue[K], vs[K], ve[K];
-        bool ok[K], hll[K];
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            const int64_t e = wb + k * stride + lane;
-            u[k] = v[k] = us[k] = ue[k] = vs[k] = ve[k] = 0;
-            ok[k] = e < P.n_edges && load_edge(P, e, u[k], v[k], us[k], ue[k], vs[k], ve[k], status);
-            hll[k] = false;
-            if (HYB && ok[k]) {
-                int32_t du, dv;
-                int64_t su, sv;
-                bool wants, both;
-                ok[k] = route(P, u[k], v[k], du, dv, su, sv, wants, both, status);
-                hll[k] = ok[k] && wants && both;
-                if (ok[k] && wants && !both) {
-                    if (P.graph_vbase && P.hll_u)  // batched: this edge's graph
-                        atomicAdd((unsigned long long*)&P.result[graph_of(P.graph_vbase, P.n_graphs, u[k])].n_fallback,
-                                  1ull);
-                    else
-                        ++fallback;
-                }
+    WARP_EDGE_LOOP(e, P.n_edges) {
+        int32_t u = 0, v = 0, us = 0, ue = 0, vs = 0, ve = 0;
+        bool ok = e < P.n_edges && load_edge(P, e, u, v, us, ue, vs, ve, status);
+        bool hll = false;
+        if (HYB && ok) {
+            int32_t du, dv;
+            int64_t su, sv;
+            bool wants, both;
+            ok = route(P, u, v, du, dv, su, sv, wants, both, status);
+            hll = ok && wants && both;
+            if (ok && wants && !both) {
+                if (P.graph_vbase && P.hll_u)  // batched: this edge's graph
+                    atomicAdd((unsigned long long*)&P.result[graph_of(P.graph_vbase, P.n_graphs, u)].n_fallback, 1ull);
+                else
+                    ++fallback;
             }
         }
-        // a run of lanes with the same table side claims its ranks with one
-        // atomic; each lane records its rank for the scatter
-        bool counted[K], side_u[K];
-        int32_t x[K], base[K];
-        int head[K], len[K];
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            counted[k] = ok[k] && !hll[k];
-            side_u[k] = (ue[k] - us[k]) >= (ve[k] - vs[k]);
-            x[k] = counted[k] ? (side_u[k] ? u[k] : v[k]) : -1 - lane;
-            lane_runs(x[k], lane, head[k], len[k]);
-        }
-#pragma unroll
-        for (int k = 0; k < K; ++k) base[k] = (counted[k] && lane == head[k]) ? atomicAdd(cnt + x[k], len[k]) : 0;
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            const int64_t e = wb + k * stride + lane;
-            base[k] = __shfl_sync(FULL, base[k], head[k]);
-            if (e < P.n_edges)
-                er[e] = counted[k] ? ((uint32_t)(base[k] + (lane - head[k])) | (side_u[k] ? 0u : kRankSideV))
-                                   : 0xFFFFFFFFu;
+        {
+            // a run of lanes with the same table side adds with one atomic
+            const bool counted = ok && !hll;
+            const int32_t x = counted ? (((ue - us) >= (ve - vs)) ? u : v) : -1 - lane;
+            int head, len;
+            lane_runs(x, lane, head, len);
+            if (counted && lane == head) atomicAdd(cnt + x, len);
         }
         if (HYB && P.hll_u) {
-#pragma unroll
-            for (int k = 0; k < K; ++k) {
-                // warp-aggregated append of the HLL-routed edges
-                const unsigned bal = __ballot_sync(FULL, hll[k]);
-                if (bal) {
-                    unsigned long long hb = 0;
-                    if (lane == 0) hb = atomicAdd(P.hll_n, (unsigned long long)__popc(bal));
-                    hb = __shfl_sync(FULL, hb, 0);
-                    if (hll[k]) {
-                        const unsigned long long pos = hb + __popc(bal & ((1u << lane) - 1u));
-                        P.hll_u[pos] = u[k];
-                        P.hll_v[pos] = v[k];
-                    }
+            // warp-aggregated append of the HLL-routed edges
+            const unsigned bal = __ballot_sync(FULL, hll);
+            if (bal) {
+                unsigned long long base = 0;
+                if (lane == 0) base = atomicAdd(P.hll_n, (unsigned long long)__popc(bal));
+                base = __shfl_sync(FULL, base, 0);
+                if (hll) {
+                    const unsigned long long pos = base + __popc(bal & ((1u << lane) - 1u));
+                    P.hll_u[pos] = u;
+                    P.hll_v[pos] = v;
                 }
             }
         }
@@ -312,55 +303,36 @@ __global__ void pair_hist_kernel(const CountParams P, int32_t* cnt, uint32_t* er
     if (HYB && P.hll_u && fallback) atomicAdd((unsigned long long*)&P.result->n_fallback, fallback);
 }
 
-// Small pairs go to px / py[off[x] + rank], hub pairs (cnth[x] > 0) to
-// py[*n_small + offh[x] + rank] (y only), with the ranks the histogram
-// recorded: no atomics here, and off / offh / cnth are only read (the hot
-// entries of the highest-degree table sides stay in L1).
-__global__ void pair_scatter_kernel(const CountParams P, const uint32_t* __restrict__ er,
-                                    const int32_t* __restrict__ off, const int32_t* __restrict__ offh,
-                                    const int32_t* __restrict__ cnth, int hub, const int32_t* n_small,
-                                    int32_t* px, int32_t* py) {
+// Small pairs go to [cursor[x]...) of px / py; with hub > 0, pairs whose x
+// has d+(x) > hub go to the hub list, py[*n_small + cursorh[x]...] (y only).
+template <bool HYB>
+__global__ void pair_scatter_kernel(const CountParams P, int32_t* cursor, int32_t* cursorh, int hub,
+                                    const int32_t* n_small, int32_t* px, int32_t* py) {
+    uint32_t status = 0;
+    const int lane = threadIdx.x & 31;
     const int64_t hbase = hub > 0 ? (int64_t)*n_small : 0;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    // four edges per thread and pass: each edge is a chain of dependent
-    // loads (rank, endpoints, bucket offsets), so keep four chains in flight
-    constexpr int K = 4;
-    for (int64_t e0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e0 < P.n_edges; e0 += K * stride) {
-        uint32_t r[K];
-        int32_t x[K], y[K];
-        bool h[K];
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            const int64_t e = e0 + k * stride;
-            r[k] = e < P.n_edges ? __ldcs(er + e) : 0xFFFFFFFFu;
-        }
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            const int64_t e = e0 + k * stride;
-            x[k] = -1;
-            y[k] = 0;
-            if (r[k] != 0xFFFFFFFFu) {
-                const int32_t u = __ldcs(P.edge_u + e), v = __ldcs(P.edge_v + e);
-                const bool side_v = (r[k] & kRankSideV) != 0;
-                x[k] = side_v ? v : u;
-                y[k] = side_v ? u : v;
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < K; ++k) h[k] = x[k] >= 0 && hub > 0 && __ldg(cnth + x[k]) > 0;
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-            if (x[k] < 0) continue;
-            const int32_t rank = (int32_t)(r[k] & ~kRankSideV);
-            if (h[k]) {
-                py[hbase + __ldg(offh + x[k]) + rank] = y[k];
+    WARP_EDGE_LOOP(e, P.n_edges) {
+        int32_t x = 0, y = 0, xl = 0;
+        const bool ok = e < P.n_edges && pair_of<HYB>(P, e, x, y, xl, status);
+        // a run of lanes with the same x claims its positions with one
+        // atomic (x's list length, hence its list, is the same for all)
+        int head, len;
+        lane_runs(ok ? x : -1 - lane, lane, head, len);
+        const bool to_hub = hub > 0 && xl > hub;
+        int32_t base = 0;
+        if (ok && lane == head) base = atomicAdd((to_hub ? cursorh : cursor) + x, len);
+        base = __shfl_sync(FULL, base, head);
+        if (ok) {
+            const int32_t pos = base + (lane - head);
+            if (to_hub) {
+                py[hbase + pos] = y;
             } else {
-                const int32_t pos = __ldg(off + x[k]) + rank;
-                px[pos] = x[k];
-                py[pos] = y[k];
+                px[pos] = x;
+                py[pos] = y;
             }
         }
     }
+    (void)status;
 }
 
 // Warp-cooperative binary-search intersection count of two sorted lists in
@@ -2115,7 +2087,6 @@ struct CountWs {
     int32_t* offh;            // n_nodes + 1
     int32_t* px;              // n_edges
     int32_t* py;              // n_edges (small pairs, then the hub list)
-    uint32_t* er;             // n_edges: each edge's pair rank in its table side's bucket (pair_hist_kernel)
     HubSeg* segs;             // max_segs
     int64_t max_segs;
     int32_t* pcol;            // padded lists in core coordinates for the hub kernels, pcap entries (null: not carved)
@@ -2152,7 +2123,6 @@ static bool carve_count(void* ws, size_t bytes, int64_t n_nodes, int64_t n_edges
     W.offh = cv.take<int32_t>(N);
     W.px = cv.take<int32_t>(E);
     W.py = cv.take<int32_t>(E);
-    W.er = cv.take<uint32_t>(E);
     // every hub x with pairs opens one segment, every HUB_SEG_MIN pairs at most one more
     W.max_segs = (int64_t)(N < E ? N : E) + (int64_t)(E / HUB_SEG_MIN) + 1;
     W.segs = cv.take<HubSeg>((size_t)W.max_segs);
@@ -2286,13 +2256,13 @@ static int grid_edges(int64_t n) {
 // Pair regrouping, part 1: histogram of table sides and its exclusive scan
 // (W.off[x] = first pair of x, W.off[n_nodes] = number of pairs).
 // With hub > 0 the histogram is split into small and hub pairs, both are
-// scanned, and the hub segments are listed.
+// scanned, and the hub segments are listed (before the scatter moves offh).
 template <bool HYB>
 static int pairs_hist_scan(const CountParams& P, const CountWs& W, int hub, int hub_seg, cudaStream_t st,
                            const int32_t* vbase = nullptr, int64_t n_graphs = 0) {
     const int64_t N = P.n_nodes + 1;
     TCHLL_CUDA(cudaMemsetAsync(W.cnt, 0, sizeof(int32_t) * N, st));
-    pair_hist_kernel<HYB><<<grid_edges(P.n_edges), 256, 0, st>>>(P, W.cnt, W.er);
+    pair_hist_kernel<HYB><<<grid_edges(P.n_edges), 256, 0, st>>>(P, W.cnt);
     TCHLL_CHECK_LAUNCH("pair_hist_kernel");
     if (hub > 0) {
         hub_split_kernel<<<grid_edges(N), 256, 0, st>>>(P.row_ptr, P.n_nodes, hub, W.cnt, W.cnth);
@@ -2313,12 +2283,12 @@ static int pairs_hist_scan(const CountParams& P, const CountWs& W, int hub, int 
     return TCHLL_OK;
 }
 
-// Part 2: scatter the pairs to the offsets the scans gave plus the ranks the
-// histogram recorded, and point Q at the small-pair list.
+// Part 2: scatter the pairs (advances W.off[x] / W.offh[x] for x < n_nodes
+// only, so the totals in [n_nodes] survive) and point Q at the small-pair list.
 template <bool HYB>
 static int pairs_scatter(const CountParams& P, const CountWs& W, int hub, CountParams& Q, cudaStream_t st) {
-    pair_scatter_kernel<<<grid_edges(P.n_edges), 256, 0, st>>>(P, W.er, W.off, W.offh, W.cnth, hub,
-                                                               W.off + P.n_nodes, W.px, W.py);
+    pair_scatter_kernel<HYB><<<grid_edges(P.n_edges), 256, 0, st>>>(P, W.off, W.offh, hub, W.off + P.n_nodes,
+                                                                   W.px, W.py);
     TCHLL_CHECK_LAUNCH("pair_scatter_kernel");
     Q = P;
     Q.edge_u = W.px;
