@@ -260,15 +260,11 @@ class Server:
         filling the budget graph by graph would call cudaMalloc for every new
         graph while requests wait (measured at 400 requests/s: p99 340 ms
         with the pools growing on demand, 24 ms with them warm)."""
-        # start from unfragmented pools: blocks cached by earlier work are
-        # cut to earlier sizes, and a new graph that fits none of them calls
-        # cudaMalloc mid-run (hundreds of calls in a 4,000-request run)
-        torch.cuda.synchronize(self.dev)
-        torch.cuda.empty_cache()
         free, _ = torch.cuda.mem_get_info(self.dev)
-        margin = 24 << 30  # the rest of the process: workspaces, default-stream work
-        for stream, want in ((self.build_stream, int(self.budget * 1.25)), (self.count_stream, int(self.budget / 16))):
-            want = min(want, free - margin)
+        margin = 8 << 30
+        for stream, want in ((self.build_stream, int(self.budget * 1.05)), (self.count_stream, int(self.budget / 16))):
+            cached = torch.cuda.memory_reserved(self.dev) - torch.cuda.memory_allocated(self.dev)
+            want = min(want, free - margin) - cached
             if want < (1 << 30):
                 continue
             with torch.cuda.stream(stream):
