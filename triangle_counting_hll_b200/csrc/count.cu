@@ -1622,6 +1622,7 @@ struct HllParams {
     int p;
     int variant;
     uint32_t lc_min;
+    int zsh;  // contiguous runs: u's mask kept in shared memory (one slot per group) when registers cannot hold it
     tchll_count_result* result;
 };
 
@@ -1764,6 +1765,7 @@ __device__ __forceinline__ double hll_estimate_from(U128 zsum, double extra, uin
 // row.  Otherwise the groups stride over the list.
 template <int L, bool ZM, bool CACHE, bool CROW>
 __global__ void __launch_bounds__(256, CROW ? 2 : (CACHE ? 3 : 4)) hll_edges_kernel(const HllParams H) {
+    extern __shared__ __align__(16) uint4 zsm[];  // with H.zsh: 256 / L slots of one zero mask each
     const int lane = threadIdx.x & 31;
     const int sub = lane & (L - 1);
     const unsigned gmask = (L == 32) ? FULL : (((1u << L) - 1u) << (lane & ~(L - 1)));
@@ -1819,6 +1821,21 @@ __global__ void __launch_bounds__(256, CROW ? 2 : (CACHE ? 3 : 4)) hll_edges_ker
                             zeros += __popc(ca[kk].x & b.x) + __popc(ca[kk].y & b.y) + __popc(ca[kk].z & b.z) +
                                      __popc(ca[kk].w & b.w);
                         }
+                    }
+                } else if (CACHE && H.zsh) {
+                    // u's mask in the group's shared-memory slot while
+                    // consecutive edges share u: each edge reads v's only
+                    uint4* zs = zsm + (size_t)(threadIdx.x / L) * nq;
+                    if (su != cached) {  // group-uniform
+                        __syncwarp(gmask);  // the group is done with the previous row
+                        for (int i = sub; i < nq; i += L) zs[i] = __ldg(za + i);
+                        __syncwarp(gmask);
+                        cached = su;
+                    }
+#pragma unroll 4
+                    for (int i = sub; i < nq; i += L) {
+                        const uint4 a = zs[i], b = __ldg(zb + i);
+                        zeros += __popc(a.x & b.x) + __popc(a.y & b.y) + __popc(a.z & b.z) + __popc(a.w & b.w);
                     }
                 } else {
 #pragma unroll 4
@@ -2187,10 +2204,26 @@ static uint32_t lc_min_for(int p) {
 }
 
 template <int L>
-static int launch_hll_edges_L(const HllParams& H, bool crow, cudaStream_t st) {
+static int launch_hll_edges_L(HllParams H, bool crow, cudaStream_t st) {
     const int grid = sm_count() * 8;
+    H.zsh = 0;
     if (H.zm && crow && L * 8 >= ((1 << H.p) >> 4)) hll_edges_kernel<L, true, true, true><<<grid, 256, 0, st>>>(H);
-    else if (H.zm && H.p >= 11) hll_edges_kernel<L, true, true, false><<<grid, 256, 0, st>>>(H);
+    else if (H.zm && H.p >= 11) {
+        // masks too large for the 4 register words per lane go to shared
+        // memory, one slot per group, while that fits 96 KB per CTA
+        const int nq = H.zst >> 2;
+        const size_t smem = nq > 4 * L ? (size_t)(256 / L) * nq * sizeof(uint4) : 0;
+        size_t bytes = 0;
+        if (smem > 0 && smem <= (96u << 10)) {
+            static size_t set[kMaxDevices] = {0};
+            const int rc = ensure_smem((const void*)hll_edges_kernel<L, true, true, false>, smem, set,
+                                       "cudaFuncSetAttribute(hll_edges_kernel)");
+            if (rc) return rc;
+            H.zsh = 1;
+            bytes = smem;
+        }
+        hll_edges_kernel<L, true, true, false><<<grid, 256, bytes, st>>>(H);
+    }
     else if (H.zm) hll_edges_kernel<L, true, false, false><<<grid, 256, 0, st>>>(H);
     else hll_edges_kernel<L, false, false, false><<<grid, 256, 0, st>>>(H);
     TCHLL_CHECK_LAUNCH("hll_edges_kernel");
