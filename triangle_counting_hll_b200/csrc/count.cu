@@ -867,13 +867,15 @@ __device__ __forceinline__ uint32_t plane_key(const int32_t* __restrict__ col, c
     return c >= kPlane ? (uint32_t)(c - kPlane) : 0xFFFFu;
 }
 
-// Within each plane the keys are ordered by the shared-memory bank of their
-// bitmap word ((key >> 5) & 31; a list is a set, so order is free): the hub
-// kernel deals consecutive 8-key units to consecutive lanes, so one load
-// instruction then mostly touches distinct banks (simulated on R-MAT: 2.5
-// instead of 3.2 shared-memory wavefronts per load).  A counting sort per
-// row and plane: 8 lanes count the 32 banks in shared memory, scan them and
-// scatter the keys; the order inside a bank is arbitrary.
+// By default the keys keep the row's order.  With bank_sort, within each
+// plane the keys are ordered by the shared-memory bank of their bitmap word
+// ((key >> 5) & 31; a list is a set, so order is free): the hub kernel deals
+// consecutive 8-key units to consecutive lanes, so one load instruction then
+// mostly touches distinct banks (R-MAT 21: 3.3 instead of 3.8 shared-memory
+// wavefronts per load, but the sort costs this pass more than the hub
+// kernel saves).  A counting sort per row and plane: 8 lanes count the 32
+// banks in shared memory, scan them and scatter the keys; the order inside a
+// bank is arbitrary; a plane of at most 8 keys is one unit and is not sorted.
 __global__ void __launch_bounds__(256) core_pad16_kernel(const int32_t* __restrict__ row_ptr, int64_t n_nodes,
                                                          int64_t nnz, const int32_t* __restrict__ col,
                                                          const int32_t* __restrict__ cidx,
